@@ -1,0 +1,367 @@
+#!/usr/bin/env python
+"""Benchmark: cell-steps/s of the leap-frog Schroedinger-Poisson step at 512^3.
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+
+Workload (ours): one 512^3 box (xmax = 5 Mpc/h, mfdm = 2.5e-24 eV, g = 0) from a
+seeded z = 50 Zel'dovich field, fixed-step mode with the reference's timestep
+rule scaled so 1000 steps reach a = 0.5.  A "step" is one full leap-frog step
+(timestep + kick + FFT + drift + iFFT + Poisson + kick, 10 kernels).  The
+headline `value` is the FP32-mixed path with psi resident in HBM; the FP64
+(drop-in) path is timed the same way beside it.  `e2e` times the public API
+with host buffers: psi uploaded from pinned memory, K steps, psi read back.
+With --gpus N > 1 (torchrun) every rank advances its own box (replicas: the
+north star keeps one box per GPU), timed as the max over ranks.
+
+--impl reference times the reference's own CPU code (oracle/_ref/BECMPI_ref,
+its unmodified sources with single-rank MPI/FFTW/GSL shims) on this host:
+rerun from a synthetic 512^3 snapshot, per-step time from the shim's
+timestamps at the two MPI_Allreduce calls of each step.
+"""
+
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import tempfile
+import threading
+import time
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+N_DEFAULT = 512
+XMAX = 5.0
+MFDM = 2.5e-24
+A0 = 1.0 / 51.0
+METRIC = "cell-steps/s at 512^3, FP32-mixed vs FP64 at <=1e-5 density err; adjoint/fwd"
+
+
+def dt_scale_for(N: int, nsteps: int = 1000, a_end: float = 0.5, xmax: float = XMAX, mfdm: float = MFDM) -> float:
+    """Multiplier C of the reference's kinetic timestep rule
+    (src/CosmoBEC_MPI.cpp:32) so that nsteps kinetic-limited steps take a from
+    1/51 to a_end."""
+    import math
+
+    m2Mpc, s2Myr = 3.086e22, 60.0 * 60.0 * 24.0 * 365.0 * 1e6
+    hbar = 6.58211928e-16 / s2Myr
+    c = 2.99792458e8 / m2Mpc * s2Myr
+    H0 = 0.677 * 100 * s2Myr / m2Mpc * 1e3
+    Om = 0.276
+    dx = 2.0 * (xmax / 0.677) / N
+    A = 4.0 / (3.0 * math.pi) * (mfdm / c**2) / hbar * dx**2
+
+    def a_after(C):
+        a = A0
+        for _ in range(nsteps):
+            a += H0 * math.sqrt(Om / a**3 + 1 - Om) * a * C * A * a * a
+            if a > 10:
+                break
+        return a
+
+    lo, hi = 1e-6, 100.0
+    for _ in range(200):
+        mid = math.sqrt(lo * hi)
+        if a_after(mid) > a_end:
+            hi = mid
+        else:
+            lo = mid
+    return math.sqrt(lo * hi)
+
+
+class ClockSampler:
+    """nvidia-smi samples during the timed region (SM clock, throttle reasons)."""
+
+    def __init__(self, device: int):
+        self.device = device
+        self.rows = []
+        self.proc = None
+
+    def __enter__(self):
+        q = ("clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.hw_slowdown,"
+             "clocks_event_reasons.hw_thermal_slowdown,clocks_event_reasons.sw_thermal_slowdown,"
+             "clocks_event_reasons.sw_power_cap")
+        try:
+            self.proc = subprocess.Popen(["nvidia-smi", "-i", str(self.device), f"--query-gpu={q}",
+                                          "--format=csv,noheader,nounits", "-lms", "200"],
+                                         stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self.t = threading.Thread(target=self._read, daemon=True)
+            self.t.start()
+        except FileNotFoundError:
+            self.proc = None
+        return self
+
+    def _read(self):
+        for line in self.proc.stdout:
+            parts = [p.strip() for p in line.split(",")]
+            if len(parts) == 7:
+                self.rows.append(parts)
+
+    def __exit__(self, *exc):
+        if self.proc:
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except subprocess.TimeoutExpired:
+                self.proc.kill()
+
+    def summary(self):
+        if not self.rows:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["unsampled"]}
+
+        def num(x):
+            try:
+                return float(x)
+            except ValueError:
+                return None
+
+        sm = [num(r[0]) for r in self.rows if num(r[0])]
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        reasons = sorted({names[i] for r in self.rows for i in range(4) if r[3 + i].lower().startswith("active")})
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": num(self.rows[0][1]),
+                "reasons": reasons, "samples": len(self.rows),
+                "power_w_max": max((num(r[2]) or 0.0) for r in self.rows)}
+
+
+def measured_peaks():
+    try:
+        with open(os.path.join(ROOT, "MEASURED_PEAKS.json")) as f:
+            return json.load(f), "measured"
+    except OSError:
+        return {"hbm_gbs": 6650.0, "bf16_tflops": 1590.0}, "fallback"
+
+
+def time_steps(sim, steps: int, warmup: int, dt_scale: float, torch):
+    """Device time of `steps` fixed-mode steps on the library's stream."""
+    stream = torch.cuda.ExternalStream(sim.stream)
+    sim.step(warmup, dt_scale)
+    sim.synchronize()
+    e0 = torch.cuda.Event(enable_timing=True)
+    e1 = torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    sim.step(steps, dt_scale)
+    e1.record(stream)
+    e1.synchronize()
+    return e0.elapsed_time(e1)
+
+
+def cpu_baseline_port(N: int, psi0, dt_scale: float):
+    """The oracle (C restatement, OpenMP on every host core) for one step at N^3."""
+    from oracle import Oracle, OracleArgs
+
+    o = Oracle(OracleArgs(res=N, mfdm=MFDM, xmax=XMAX))
+    o.set_psi(psi0, A0)
+    t = time.perf_counter()
+    o.run_fixed(1, dt_scale)
+    dt = time.perf_counter() - t
+    o.close()
+    return {"value": N**3 / dt, "unit": "cell-steps/s", "cores": Oracle.num_threads(), "kind": "port",
+            "sample": f"1 leap-frog step of the {N}^3 workload ({dt:.1f} s)"}
+
+
+def run_ours(args):
+    import numpy as np
+    import torch
+
+    import ifdm_code_b200 as ifdm
+    from ifdm_code_b200.synthetic_ic import zeldovich_psi
+
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    dist = None
+    if world > 1:
+        import datetime
+
+        import torch.distributed as dist
+
+        torch.cuda.set_device(local)
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=600))
+    torch.cuda.set_device(local)
+    N = args.res
+    K, W = args.steps, args.warmup
+    C = dt_scale_for(N)
+    psi0 = zeldovich_psi(N, xmax=XMAX, seed=rank, a=A0, mfdm=MFDM)
+    peaks, peak_kind = measured_peaks()
+    hbm = float(peaks["hbm_gbs"])
+
+    def barrier():
+        if dist:
+            dist.barrier()
+        torch.cuda.synchronize()
+
+    def max_over_ranks(v):
+        if not dist:
+            return v
+        t = torch.tensor([v], dtype=torch.float64, device="cuda")
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        return float(t.item())
+
+    res = {}
+    for prec in ("fp32", "fp64"):
+        sim = ifdm.Simulation(MFDM, 0.0, XMAX, N, precision=prec, device=local)
+        sim.set_psi(psi0, A0)
+        sim.step(W, C)
+        sim.synchronize()
+        barrier()
+        clk = ClockSampler(local) if prec == "fp32" else None
+        if clk:
+            clk.__enter__()
+        ms = time_steps(sim, K, 0, C, torch)
+        if clk:
+            clk.__exit__()
+        barrier()
+        ms = max_over_ranks(ms)
+        prof = sim.profile_passes(max(3, min(10, K)), C)
+        pb = sim.pass_bytes()
+        st = sim.state()
+        res[prec] = dict(ms=ms, prof=prof, bytes=pb, state=st, clocks=clk.summary() if clk else None)
+        sim.close()
+        del sim
+        torch.cuda.synchronize()
+
+    # end to end through the C ABI with host buffers (pinned)
+    pin_in = torch.from_numpy(psi0.view(np.float64)).pin_memory()
+    pin_out = torch.empty_like(pin_in).pin_memory()
+    sim = ifdm.Simulation(MFDM, 0.0, XMAX, N, precision="fp32", device=local)
+    sim.set_psi(pin_in.numpy().view(np.complex128), A0)
+    sim.step(W, C)
+    sim.synchronize()
+    barrier()
+    t0 = time.perf_counter()
+    sim.set_psi(pin_in.numpy().view(np.complex128), A0)
+    sim.step(K, C)
+    sim.get_psi(out=pin_out.numpy().view(np.complex128).reshape(N, N, N))
+    e2e_s = time.perf_counter() - t0
+    sim.close()
+    e2e_s = max_over_ranks(e2e_s)
+
+    cells = float(N) ** 3
+    value = world * cells * K / (res["fp32"]["ms"] / 1e3)
+    fp64_value = world * cells * K / (res["fp64"]["ms"] / 1e3)
+    e2e_value = world * cells * K / e2e_s
+
+    def roofline(r):
+        names = list(r["prof"].keys())
+        ms = [r["prof"][n] for n in names]
+        i = max(range(1, len(ms)), key=lambda j: ms[j])
+        achieved = r["bytes"][i] / (ms[i] / 1e3) / 1e9
+        step_bytes = sum(r["bytes"])
+        return {"bound": "hbm", "kernel": names[i], "achieved": round(achieved, 1), "peak": hbm, "unit": "GB/s",
+                "frac": round(achieved / hbm, 4), "traffic": None, "peak_kind": peak_kind,
+                "step_bytes_per_cell": step_bytes / cells,
+                "step_achieved_gbs": round(step_bytes / (sum(ms) / 1e3) / 1e9, 1),
+                "passes_ms": {n: round(v, 4) for n, v in zip(names, ms)},
+                "passes_frac": {n: round(b / (v / 1e3) / 1e9 / hbm, 3) for n, v, b in zip(names, ms, r["bytes"])
+                                if b > 0}}
+
+    out = {
+        "metric": METRIC,
+        "value": value,
+        "unit": "cell-steps/s",
+        "n_gpus": world,
+        "steps": K,
+        "warmup": W,
+        "ms_per_step": res["fp32"]["ms"] / K,
+        "higher_is_better": True,
+        "scaling": "weak",
+        "vs_baseline": None,
+        "dtype": "f32",
+        "data": "synthetic",
+        "config": {"workload": f"{N}^3 leap-frog step, xmax=5 Mpc/h, mfdm=2.5e-24 eV, g=0, z=50 Zel'dovich IC, "
+                               f"fixed-step dt_scale={C:.4f} (1000 steps to a=0.5)",
+                   "res": N, "parallelism": f"replicas x{world}" if world > 1 else "1 box",
+                   "l2": "inputs larger than L2 (psi fp32 = %.1f GB)" % (8 * cells / 1e9)},
+        "fp64": {"value": fp64_value, "unit": "cell-steps/s", "ms_per_step": res["fp64"]["ms"] / K,
+                 "fp32_over_fp64": value / fp64_value, "roofline": roofline(res["fp64"])},
+        "roofline": roofline(res["fp32"]),
+        "e2e": {"value": e2e_value, "unit": "cell-steps/s", "h2d_bytes_per_step": 16 * cells / K,
+                "d2h_bytes_per_step": 16 * cells / K,
+                "note": f"set_psi from pinned host complex128, {K} steps, get_psi to pinned host, per step = /K"},
+        "gpu_launches": 10 * K,
+        "clocks": res["fp32"]["clocks"],
+    }
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        out["cpu_baseline"] = cpu_baseline_port(N, psi0, C)
+    if dist:
+        dist.destroy_process_group()
+    if rank == 0:
+        print(json.dumps(out))
+
+
+def run_reference(args):
+    """The reference's own code on the host cores (rank 0 only)."""
+    import numpy as np
+
+    rank = int(os.environ.get("RANK", "0"))
+    if rank != 0:
+        return
+    from ifdm_code_b200.synthetic_ic import zeldovich_psi
+    from oracle import ref_binary
+
+    N = args.res
+    binary = ref_binary()
+    if binary is None:
+        print(json.dumps({"impl": "reference", "unavailable": "oracle/_ref/BECMPI_ref was not built"}))
+        return
+    K = max(1, min(args.steps, args.ref_max_steps))
+    W = 1
+    with tempfile.TemporaryDirectory() as d:
+        psi0 = zeldovich_psi(N, xmax=XMAX, seed=0, a=A0, mfdm=MFDM)
+        xm = XMAX / 0.677
+        x = xm / N - xm + np.arange(N) * (2 * xm / N)
+        with open(os.path.join(d, "output1.dat"), "wb") as f:
+            np.array([MFDM, 0.0, A0], dtype=np.float64).tofile(f)
+            x.astype(np.float64).tofile(f)
+            psi0.tofile(f)
+        del psi0
+        tf = os.path.join(d, "steps.txt")
+        env = dict(os.environ, IFDM_SHIM_TIMING=tf)
+        # rerun from output1.dat; t_write larger than the run so only the last
+        # step writes (that step is not timed)
+        cmd = [binary, str(MFDM), "0", str(XMAX), str(N), "1000000", str(1 + W + K + 1), "1", d + "/", d + "/", "1"]
+        subprocess.run(cmd, env=env, capture_output=True, text=True, check=True)
+        ts = [float(v) for v in open(tf).read().split()]
+    starts = ts[0::2]
+    dts = [b - a for a, b in zip(starts[:-1], starts[1:])][W:W + K]
+    sec = statistics.mean(dts)
+    value = float(N) ** 3 / sec
+    cores = os.cpu_count()
+    print(json.dumps({
+        "impl": "reference", "metric": METRIC, "value": value, "unit": "cell-steps/s", "n_gpus": 0,
+        "steps": len(dts), "warmup": W, "ms_per_step": sec * 1e3, "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+        "config": {"workload": f"{N}^3 leap-frog step (reference loop, rerun from a synthetic snapshot)",
+                   "res": N},
+        "cpu_baseline": {"value": value, "unit": "cell-steps/s", "cores": cores, "kind": "reference",
+                         "sample": f"{len(dts)} timed steps after {W} warm-up at {N}^3; FFTs on {cores} OpenMP "
+                                   "threads (shim), pointwise loops on 1 thread as one MPI rank runs them"},
+        "e2e": {"value": value, "unit": "cell-steps/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }))
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=50)
+    ap.add_argument("--warmup", type=int, default=5)
+    ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
+    ap.add_argument("--res", type=int, default=N_DEFAULT)
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--ref-max-steps", type=int, default=3,
+                    help="bound on timed reference steps (each is ~tens of seconds at 512^3)")
+    args = ap.parse_args()
+    if args.warmup < 3 and args.impl == "ours":
+        args.warmup = 3
+    if args.impl == "reference":
+        run_reference(args)
+    else:
+        run_ours(args)
+
+
+if __name__ == "__main__":
+    main()

@@ -1,0 +1,192 @@
+// fft_engine.cuh -- shared-memory Stockham FFT over a tile of lines, sm_100a.
+//
+// A tile holds L independent lines of length N in shared memory, element
+// (line l, index n) at sm[n * LP + l] with LP = L + 1.  The line index is the
+// fastest-varying one, so the 8 (FP64) or 16 (FP32) threads of one
+// shared-memory phase always touch consecutive words: butterfly reads and
+// writes are conflict-free whatever the stage stride, and the odd pitch also
+// makes the transposing copies of contiguous z-lines conflict-free.
+//
+// Thread (l = tid % L, t = tid / L) owns E = N / T elements of line l; a
+// radix-R stage runs E / R butterflies per thread (Stockham autosort, so no
+// bit reversal pass).  Twiddles come from a per-size table of
+// exp(-2 pi i m / N) built on the host in long double and rounded once.
+#pragma once
+
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+namespace ifdm {
+
+// ---------------------------------------------------------------- complex --
+template <typename R> struct CxT;
+template <> struct CxT<double> { using T = double2; };
+template <> struct CxT<float> { using T = float2; };
+template <typename R> using cx = typename CxT<R>::T;
+
+__device__ __forceinline__ double2 mkc(double a, double b) { return make_double2(a, b); }
+__device__ __forceinline__ float2 mkc(float a, float b) { return make_float2(a, b); }
+__device__ __forceinline__ double2 operator+(double2 a, double2 b) { return mkc(a.x + b.x, a.y + b.y); }
+__device__ __forceinline__ double2 operator-(double2 a, double2 b) { return mkc(a.x - b.x, a.y - b.y); }
+__device__ __forceinline__ float2 operator+(float2 a, float2 b) { return mkc(a.x + b.x, a.y + b.y); }
+__device__ __forceinline__ float2 operator-(float2 a, float2 b) { return mkc(a.x - b.x, a.y - b.y); }
+template <typename C> __device__ __forceinline__ C cmul(C a, C b) {
+    return mkc(a.x * b.x - a.y * b.y, a.x * b.y + a.y * b.x);
+}
+template <typename C, typename S> __device__ __forceinline__ C cscale(C a, S s) { return mkc(a.x * s, a.y * s); }
+template <typename C> __device__ __forceinline__ C cconj(C a) { return mkc(a.x, -a.y); }
+// multiply by -i (DIR = -1) or +i (DIR = +1)
+template <int DIR, typename C> __device__ __forceinline__ C mul_i(C a) {
+    return DIR < 0 ? mkc(a.y, -a.x) : mkc(-a.y, a.x);
+}
+template <typename C> __device__ __forceinline__ auto cnorm2(C a) { return a.x * a.x + a.y * a.y; }
+
+// ------------------------------------------------------------- radix plans --
+// Radix sequence per transform length; every radix divides E (elements per
+// thread), so a stage is E/R whole butterflies per thread.
+template <int N> struct Plan;
+template <> struct Plan<8> { static constexpr int E = 8, NST = 1; static constexpr int R[1] = {8}; };
+template <> struct Plan<16> { static constexpr int E = 8, NST = 2; static constexpr int R[2] = {8, 2}; };
+template <> struct Plan<24> { static constexpr int E = 12, NST = 3; static constexpr int R[3] = {4, 3, 2}; };
+template <> struct Plan<32> { static constexpr int E = 8, NST = 2; static constexpr int R[2] = {8, 4}; };
+template <> struct Plan<48> { static constexpr int E = 12, NST = 3; static constexpr int R[3] = {4, 4, 3}; };
+template <> struct Plan<64> { static constexpr int E = 8, NST = 2; static constexpr int R[2] = {8, 8}; };
+template <> struct Plan<96> { static constexpr int E = 12, NST = 4; static constexpr int R[4] = {4, 4, 3, 2}; };
+template <> struct Plan<128> { static constexpr int E = 8, NST = 3; static constexpr int R[3] = {8, 8, 2}; };
+template <> struct Plan<256> { static constexpr int E = 8, NST = 3; static constexpr int R[3] = {8, 8, 4}; };
+template <> struct Plan<512> { static constexpr int E = 8, NST = 3; static constexpr int R[3] = {8, 8, 8}; };
+
+// ------------------------------------------------------------- butterflies --
+template <int RAD, int DIR> struct Bfly;
+
+template <int DIR> struct Bfly<2, DIR> {
+    template <typename C> __device__ __forceinline__ static void run(C *v) {
+        C a = v[0], b = v[1];
+        v[0] = a + b;
+        v[1] = a - b;
+    }
+};
+
+template <int DIR> struct Bfly<4, DIR> {
+    template <typename C> __device__ __forceinline__ static void run(C *v) {
+        C s02 = v[0] + v[2], d02 = v[0] - v[2];
+        C s13 = v[1] + v[3], d13 = mul_i<DIR>(v[1] - v[3]);
+        v[0] = s02 + s13;
+        v[2] = s02 - s13;
+        v[1] = d02 + d13;
+        v[3] = d02 - d13;
+    }
+};
+
+template <int DIR> struct Bfly<3, DIR> {
+    template <typename C> __device__ __forceinline__ static void run(C *v) {
+        using R = decltype(v[0].x);
+        const R h = R(0.5);
+        const R s3 = R(0.86602540378443864676372317075294);  // sqrt(3)/2
+        C t1 = v[1] + v[2];
+        C t2 = v[0] - cscale(t1, h);
+        C t3 = cscale(mul_i<DIR>(v[1] - v[2]), s3);
+        v[0] = v[0] + t1;
+        v[1] = t2 + t3;
+        v[2] = t2 - t3;
+    }
+};
+
+template <int DIR> struct Bfly<8, DIR> {
+    template <typename C> __device__ __forceinline__ static void run(C *v) {
+        using R = decltype(v[0].x);
+        const R q = R(0.70710678118654752440084436210485);  // 1/sqrt(2)
+        C a0 = v[0] + v[4], a1 = v[0] - v[4];
+        C a2 = v[2] + v[6], a3 = mul_i<DIR>(v[2] - v[6]);
+        C a4 = v[1] + v[5], a5 = v[1] - v[5];
+        C a6 = v[3] + v[7], a7 = mul_i<DIR>(v[3] - v[7]);
+        C b0 = a0 + a2, b2 = a0 - a2, b1 = a1 + a3, b3 = a1 - a3;
+        C c0 = a4 + a6, c2 = a4 - a6, c1 = a5 + a7, c3 = a5 - a7;
+        // c1 *= w8, c2 *= w8^2 = -/+i, c3 *= w8^3 ; w8 = (1 -/+ i)/sqrt2
+        C w1, w3;
+        if (DIR < 0) {
+            w1 = mkc((c1.x + c1.y) * q, (c1.y - c1.x) * q);
+            w3 = mkc((c3.y - c3.x) * q, -(c3.x + c3.y) * q);
+        } else {
+            w1 = mkc((c1.x - c1.y) * q, (c1.x + c1.y) * q);
+            w3 = mkc(-(c3.x + c3.y) * q, (c3.x - c3.y) * q);
+        }
+        C w2 = mul_i<DIR>(c2);
+        v[0] = b0 + c0;
+        v[4] = b0 - c0;
+        v[1] = b1 + w1;
+        v[5] = b1 - w1;
+        v[2] = b2 + w2;
+        v[6] = b2 - w2;
+        v[3] = b3 + w3;
+        v[7] = b3 - w3;
+    }
+};
+
+// twiddle exp(DIR * 2 pi i m / N) from the forward table
+template <int DIR, typename C> __device__ __forceinline__ C twiddle(const C *__restrict__ tw, int m) {
+    C w = __ldg(tw + m);
+    return DIR < 0 ? w : cconj(w);
+}
+
+// One Stockham stage: radix RAD, NS = product of the previous radices.
+template <typename C, int N, int E, int DIR, int L, int LP, int RAD, int NS>
+__device__ __forceinline__ void stockham_stage(C *sm, const C *__restrict__ tw, int l, int t, bool active) {
+    constexpr int T = N / E;
+    constexpr int NB = E / RAD;
+    constexpr int STRIDE = N / RAD;
+    constexpr int TWSTEP = N / (NS * RAD);
+    C v[E];
+    if (active) {
+#pragma unroll
+        for (int b = 0; b < NB; ++b) {
+            const int j = t + T * b;
+            const int k = j % NS;
+#pragma unroll
+            for (int r = 0; r < RAD; ++r) {
+                C a = sm[(j + r * STRIDE) * LP + l];
+                if (NS > 1 && r > 0) a = cmul(a, twiddle<DIR>(tw, k * r * TWSTEP));
+                v[b * RAD + r] = a;
+            }
+            Bfly<RAD, DIR>::run(&v[b * RAD]);
+        }
+    }
+    __syncthreads();
+    if (active) {
+#pragma unroll
+        for (int b = 0; b < NB; ++b) {
+            const int j = t + T * b;
+            const int k = j % NS;
+            const int base = (j / NS) * NS * RAD + k;
+#pragma unroll
+            for (int r = 0; r < RAD; ++r) sm[(base + r * NS) * LP + l] = v[b * RAD + r];
+        }
+    }
+    __syncthreads();
+}
+
+template <typename C, int N, int DIR, int L, int LP, int S, int NS>
+struct StageLoop {
+    __device__ __forceinline__ static void run(C *sm, const C *__restrict__ tw, int l, int t, bool active) {
+        if constexpr (S < Plan<N>::NST) {
+            constexpr int RAD = Plan<N>::R[S];
+            stockham_stage<C, N, Plan<N>::E, DIR, L, LP, RAD, NS>(sm, tw, l, t, active);
+            StageLoop<C, N, DIR, L, LP, S + 1, NS * RAD>::run(sm, tw, l, t, active);
+        }
+    }
+};
+
+// Transform all L lines of the tile in place.  `nthreads` = blockDim.x; lines
+// are processed by threads tid < L * (N / E); the rest only join the barriers.
+// Caller must __syncthreads() before (tile written) -- this routine leaves the
+// tile synced.
+template <typename C, int N, int DIR, int L, int LP>
+__device__ __forceinline__ void fft_tile(C *sm, const C *__restrict__ tw) {
+    constexpr int T = N / Plan<N>::E;
+    const int tid = threadIdx.x;
+    const int l = tid % L;
+    const int t = tid / L;
+    StageLoop<C, N, DIR, L, LP, 0, 1>::run(sm, tw, l, t, t < T);
+}
+
+}  // namespace ifdm

@@ -1,0 +1,419 @@
+// ifdm_api.cpp -- the C ABI of include/ifdm.h.
+#include "../../include/ifdm.h"
+
+#include <cuda_runtime.h>
+
+#include <cmath>
+#include <cstdio>
+#include <cstdlib>
+#include <cstring>
+#include <memory>
+#include <string>
+#include <vector>
+
+#include "ic_pipeline.hpp"
+#include "io.hpp"
+#include "physics.hpp"
+#include "step_engine.hpp"
+
+using namespace ifdm;
+
+struct ifdm_ctx {
+    ifdm_params p{};
+    std::string opath, icpath, err;
+    int N = 0;
+    // globals of main() (src/CosmoBEC_MPI.cpp:329-339) and Params (src/struct3D.h:43-87)
+    double mfdm = 0, mfdm_solar = 0, g = 0, xmax = 0, dx = 0;
+    std::vector<double> x;
+    double a0 = 0, rhoc = 0;
+    cudaStream_t stream = nullptr;
+    StepEngine eng;
+    bool have_psi = false;
+    double *d_out = nullptr;   // complex128 N^3 device staging for outputs
+    double *h_out = nullptr;   // pinned host staging
+    size_t h_out_bytes = 0;
+};
+
+static int fail(ifdm_ctx *c, int code, const std::string &msg) {
+    if (c) c->err = msg;
+    return code;
+}
+
+#define CTX_CUDA(c, expr)                                                                              \
+    do {                                                                                               \
+        cudaError_t e_ = (expr);                                                                       \
+        if (e_ != cudaSuccess) return fail(c, IFDM_ERR_CUDA, std::string(#expr) + ": " + cudaGetErrorString(e_)); \
+    } while (0)
+
+#define CTX_STR(c, code, expr)                        \
+    do {                                              \
+        std::string s_ = (expr);                      \
+        if (!s_.empty()) return fail(c, code, s_);    \
+    } while (0)
+
+extern "C" {
+
+void ifdm_params_default(ifdm_params *p) {
+    std::memset(p, 0, sizeof(*p));
+    p->precision = IFDM_FP64;
+    p->ic_mode = IFDM_IC_REF1;
+    p->t_write = 1;
+    p->opath = "";
+    p->icpath = "";
+}
+
+int ifdm_params_from_argv(int argc, char **argv, ifdm_params *p) {
+    if (argc != 11) return IFDM_ERR_ARGS;
+    ifdm_params_default(p);
+    p->mfdm = std::atof(argv[1]);
+    p->g = std::atof(argv[2]);
+    p->xmax = std::atof(argv[3]);
+    p->res = std::atoi(argv[4]);
+    p->t_write = (int)std::atof(argv[5]);
+    p->t_stop = (int)(unsigned)std::atof(argv[6]);
+    p->ti = (int)std::atof(argv[7]);
+    p->opath = argv[8];
+    p->icpath = argv[9];
+    p->rerun = (std::atof(argv[10]) == 1) ? 1 : 0;
+    return IFDM_OK;
+}
+
+int ifdm_supported_res(int res, int precision) {
+    (void)precision;
+    return supported_n(res) ? 1 : 0;
+}
+
+int ifdm_create(const ifdm_params *p, ifdm_ctx **out) {
+    if (!p || !out) return IFDM_ERR_ARGS;
+    *out = nullptr;
+    std::unique_ptr<ifdm_ctx> c(new ifdm_ctx);
+    c->p = *p;
+    c->opath = p->opath ? p->opath : "";
+    c->icpath = p->icpath ? p->icpath : "";
+    c->p.opath = c->opath.c_str();
+    c->p.icpath = c->icpath.c_str();
+    if (!supported_n(p->res)) {
+        *out = c.release();
+        return fail(*out, IFDM_ERR_UNSUPPORTED, "res " + std::to_string(p->res) + " has no compiled FFT plan");
+    }
+    if (p->precision != IFDM_FP64 && p->precision != IFDM_FP32) {
+        *out = c.release();
+        return fail(*out, IFDM_ERR_ARGS, "precision must be IFDM_FP64 or IFDM_FP32");
+    }
+    using namespace phys;
+    c->N = p->res;
+    c->mfdm = p->mfdm;
+    c->mfdm_solar = p->mfdm * kg2eV / kg2solar;
+    c->g = p->g / (pow(cm2Mpc, 3));
+    c->xmax = p->xmax / h_0;
+    const unsigned res = (unsigned)p->res;
+    c->dx = 2.0 * c->xmax / res;
+    c->x.resize(res);
+    for (size_t i = 0; i < res; ++i) c->x[i] = c->xmax / res - c->xmax + i * (2.0 * c->xmax / res);
+    ifdm_ctx *raw = c.release();
+    *out = raw;
+    CTX_CUDA(raw, cudaSetDevice(p->device));
+    CTX_CUDA(raw, cudaStreamCreateWithFlags(&raw->stream, cudaStreamNonBlocking));
+    EngineConfig ec;
+    ec.N = raw->N;
+    ec.precision = p->precision;
+    ec.mfdm = raw->mfdm;
+    ec.g = raw->g;
+    ec.xmax = raw->xmax;
+    ec.dx = raw->dx;
+    ec.mfdm_solar = raw->mfdm_solar;
+    CTX_STR(raw, IFDM_ERR_CUDA, raw->eng.init(ec, raw->stream));
+    return IFDM_OK;
+}
+
+void ifdm_destroy(ifdm_ctx *c) {
+    if (!c) return;
+    if (c->stream) cudaStreamSynchronize(c->stream);
+    cudaFree(c->d_out);
+    if (c->h_out) cudaFreeHost(c->h_out);
+    if (c->stream) cudaStreamDestroy(c->stream);
+    delete c;
+}
+
+const char *ifdm_last_error(const ifdm_ctx *c) { return c ? c->err.c_str() : "null context"; }
+
+void *ifdm_stream(ifdm_ctx *c) { return c ? (void *)c->stream : nullptr; }
+
+int ifdm_synchronize(ifdm_ctx *c) {
+    if (!c) return IFDM_ERR_ARGS;
+    CTX_CUDA(c, cudaStreamSynchronize(c->stream));
+    return IFDM_OK;
+}
+
+static int ensure_out(ifdm_ctx *c) {
+    if (!c->d_out) CTX_CUDA(c, cudaMalloc(&c->d_out, c->eng.n3() * 2 * sizeof(double)));
+    return IFDM_OK;
+}
+
+int ifdm_set_psi(ifdm_ctx *c, const double *psi, double a, double rhoc) {
+    if (!c || !psi) return IFDM_ERR_ARGS;
+    c->a0 = a;
+    c->rhoc = rhoc > 0 ? rhoc : phys::rhoc;
+    cudaPointerAttributes attr{};
+    const bool dev = cudaPointerGetAttributes(&attr, psi) == cudaSuccess && attr.type == cudaMemoryTypeDevice;
+    cudaGetLastError();
+    CTX_STR(c, IFDM_ERR_CUDA, c->eng.load_psi(psi, dev, a, c->rhoc));
+    c->have_psi = true;
+    return IFDM_OK;
+}
+
+// psi of the current state into a host buffer; which: 1 snapshot kick, 2 pending kick
+static int psi_to_host(ifdm_ctx *c, double *host, int which) {
+    if (ensure_out(c)) return IFDM_ERR_CUDA;
+    CTX_STR(c, IFDM_ERR_CUDA, c->eng.psi_out(c->d_out, which));
+    CTX_CUDA(c, cudaMemcpyAsync(host, c->d_out, c->eng.n3() * 2 * sizeof(double), cudaMemcpyDeviceToHost, c->stream));
+    CTX_CUDA(c, cudaStreamSynchronize(c->stream));
+    return IFDM_OK;
+}
+
+int ifdm_get_psi(ifdm_ctx *c, double *psi) {
+    if (!c || !psi) return IFDM_ERR_ARGS;
+    if (!c->have_psi) return fail(c, IFDM_ERR_STATE, "no wave function loaded");
+    return psi_to_host(c, psi, 2);
+}
+
+int ifdm_get_phi(ifdm_ctx *c, double *phi) {
+    if (!c || !phi) return IFDM_ERR_ARGS;
+    if (!c->have_psi) return fail(c, IFDM_ERR_STATE, "no wave function loaded");
+    if (ensure_out(c)) return IFDM_ERR_CUDA;
+    CTX_STR(c, IFDM_ERR_CUDA, c->eng.phi_out(c->d_out));
+    CTX_CUDA(c, cudaMemcpyAsync(phi, c->d_out, c->eng.n3() * sizeof(double), cudaMemcpyDeviceToHost, c->stream));
+    CTX_CUDA(c, cudaStreamSynchronize(c->stream));
+    return IFDM_OK;
+}
+
+int ifdm_get_state(ifdm_ctx *c, ifdm_state *out) {
+    if (!c || !out) return IFDM_ERR_ARGS;
+    TState t{};
+    CTX_STR(c, IFDM_ERR_CUDA, c->eng.read_state(t));
+    out->a = t.a;
+    out->dt_KE = t.dt_KE;
+    out->dt_PE = t.dt_PE;
+    out->dt_QI = t.dt_QI;
+    out->max_phi = t.maxphi;
+    out->max_rho = t.maxrho;
+    out->rhoc = c->rhoc;
+    out->steps = t.steps;
+    out->criterion = t.crit;
+    out->device_error = t.err;
+    return IFDM_OK;
+}
+
+static int write_snapshot_which(ifdm_ctx *c, int t, int which, double a) {
+    const size_t n3 = c->eng.n3();
+    const size_t bytes = n3 * 2 * sizeof(double);
+    if (c->h_out_bytes < bytes) {
+        if (c->h_out) cudaFreeHost(c->h_out);
+        c->h_out = nullptr;
+        c->h_out_bytes = 0;
+        CTX_CUDA(c, cudaMallocHost(&c->h_out, bytes));
+        c->h_out_bytes = bytes;
+    }
+    int rc = psi_to_host(c, c->h_out, which);
+    if (rc) return rc;
+    const double gg = c->g * (pow(phys::cm2Mpc, 3));
+    CTX_STR(c, IFDM_ERR_IO, write_snapshot(snapshot_path(c->opath, t), c->mfdm, gg, a, c->x, c->h_out, n3));
+    return IFDM_OK;
+}
+
+int ifdm_write_snapshot(ifdm_ctx *c, int t) {
+    if (!c) return IFDM_ERR_ARGS;
+    if (!c->have_psi) return fail(c, IFDM_ERR_STATE, "no wave function loaded");
+    TState st{};
+    CTX_STR(c, IFDM_ERR_CUDA, c->eng.read_state(st));
+    return write_snapshot_which(c, t, 2, st.steps ? st.a : c->a0);
+}
+
+int ifdm_load_snapshot(ifdm_ctx *c, int t) {
+    if (!c) return IFDM_ERR_ARGS;
+    const size_t n3 = c->eng.n3();
+    std::vector<double> psi(2 * n3);
+    double a = 0;
+    std::vector<double> x;
+    CTX_STR(c, IFDM_ERR_IO, read_snapshot(snapshot_path(c->icpath, t), c->N, &a, &x, psi.data()));
+    c->x = x;  // read_rerun overwrites par.x (src/gadget_IC.h:735)
+    return ifdm_set_psi(c, psi.data(), a, phys::rhoc);
+}
+
+int ifdm_load_ic(ifdm_ctx *c) {
+    if (!c) return IFDM_ERR_ARGS;
+    using namespace phys;
+    const int N = c->N;
+    IcInput in;
+    in.N = N;
+    GadgetHeader hd{};
+    double rhoc = 0, a = 0;
+    const int tot_chunks = 4;  // src/gadget_IC.h:610
+    for (int chunk = 0; chunk < tot_chunks; ++chunk) {
+        std::vector<float> pos, vel;
+        CTX_STR(c, IFDM_ERR_IO, read_gadget_chunk(c->icpath + "." + std::to_string(chunk), &hd, &pos, &vel));
+        if (c->p.verbose)
+            std::printf("read file from %s.%d\nnpart = %d\nmass = %g\na = %g\nredshift? = %g\nBoxSize = %g\nh = %g \n",
+                        c->icpath.c_str(), chunk, hd.npart[1], hd.mass[1], hd.time, hd.redshift, hd.BoxSize,
+                        hd.HubbleParam);
+        // src/gadget_IC.h:309-314
+        if (!(std::fabs(hd.BoxSize - 2 * c->xmax * 1e3 * h_0) < 0.001)) {
+            char msg[256];
+            std::snprintf(msg, sizeof msg, "ERROR: Boxsize of IC is different to xmax in Simulation !%g vs %g",
+                          2 * c->xmax * 1e3 / h_0, hd.BoxSize);
+            return fail(c, IFDM_ERR_BOXSIZE, msg);
+        }
+        hd.mass[1] *= 1e10;
+        a = hd.time;
+        rhoc = tot_chunks * hd.npart[1] * hd.mass[1] / pow(hd.BoxSize, 3) * pow(1e3, 3) * pow(h_0, 2);
+        const double Lg = hd.BoxSize / N;
+        const long n = hd.npart[1];
+        if (c->p.ic_mode == IFDM_IC_REF1) {
+            // one rank: trailing particles beyond the last cell centre are rank
+            // 0's left ghosts and also its own (src/gadget_IC.h:445-448,
+            // :496-502), then numpart + 1 owned particles, the extra one zero
+            // (src/gadget_IC.h:431-432)
+            const double xg_last = (N - 1) * Lg + 0.5 * Lg;
+            long lg = 0;
+            for (long pn = n - 1; pn > 0; pn--) {
+                if (xg_last < pos[3 * pn]) lg++;
+                else break;
+            }
+            in.pos.insert(in.pos.end(), pos.end() - 3 * lg, pos.end());
+            in.vel.insert(in.vel.end(), vel.end() - 3 * lg, vel.end());
+            in.pos.insert(in.pos.end(), pos.begin(), pos.end());
+            in.vel.insert(in.vel.end(), vel.begin(), vel.end());
+            for (int q = 0; q < 3; ++q) {
+                in.pos.push_back(0.f);
+                in.vel.push_back(0.f);
+            }
+        } else {
+            in.pos.insert(in.pos.end(), pos.begin(), pos.end());
+            in.vel.insert(in.vel.end(), vel.begin(), vel.end());
+        }
+        in.Lg = Lg;
+        in.box = hd.BoxSize;
+    }
+    in.pmass = hd.mass[1];
+    in.L3 = pow(in.Lg, 3);
+    in.a = a;
+    in.xmax = c->xmax;
+    in.dx = c->dx;
+    in.mfdm_solar = c->mfdm_solar;
+    in.kf = c->mfdm / pow(phys::c, 2) / hbar;
+    in.uc_rho = pow(h_0, 2) * pow(1e3, 3);
+    in.uc_vel = 1e3 / m2Mpc * s2Myr;
+    in.stream = c->stream;
+    if (ensure_out(c)) return IFDM_ERR_CUDA;
+    std::vector<float> vx;
+    CTX_STR(c, IFDM_ERR_CUDA, ic_pipeline(in, c->d_out, &vx));
+    CTX_STR(c, IFDM_ERR_IO, write_voutput(c->opath + "voutput.dat", vx.data(), vx.size()));
+    return ifdm_set_psi(c, c->d_out, a, rhoc);
+}
+
+int ifdm_step(ifdm_ctx *c, int nsteps, double dt_scale) {
+    if (!c || nsteps < 0) return IFDM_ERR_ARGS;
+    if (!c->have_psi) return fail(c, IFDM_ERR_STATE, "no wave function loaded");
+    CTX_STR(c, IFDM_ERR_CUDA, c->eng.step(nsteps, dt_scale));
+    return IFDM_OK;
+}
+
+// Simulation (src/CosmoBEC_MPI.cpp:183-310)
+int ifdm_run(ifdm_ctx *c) {
+    if (!c) return IFDM_ERR_ARGS;
+    if (!c->have_psi) return fail(c, IFDM_ERR_STATE, "no wave function loaded");
+    const bool v = c->p.verbose != 0;
+    int write_num = 0;
+    int write_sten_counter = 2;
+    for (int tn = c->p.ti; tn < c->p.t_stop; ++tn) {
+        const double a_prev = [&] {
+            TState t{};
+            c->eng.read_state(t);
+            return t.steps ? t.a : c->a0;
+        }();
+        CTX_STR(c, IFDM_ERR_CUDA, c->eng.timestep_only(1.0));
+        TState st{};
+        CTX_STR(c, IFDM_ERR_CUDA, c->eng.read_state(st));
+        if (st.err) return fail(c, IFDM_ERR_DEVICE, "device quadrature hit its interval limit");
+        const double a = st.a;
+        if (v) {
+            std::printf(" max dt_KE = %g max dt_PE = %g max dt_QI = %g\n", st.cand_KE, st.cand_PE, st.cand_QI);
+            std::printf("ai = %g a_next = %g da = %g n = %d ", a_prev, a, st.da, st.crit);
+        }
+        int rc = IFDM_OK;
+        bool stop = false;
+        if (a > 1) {
+            rc = write_snapshot_which(c, 999999, 1, a);
+            if (v) std::printf("write z = 0 at step%d\n", tn + 1);
+            write_num++;
+            stop = true;
+        } else if (a > 0.714 && write_num == 4) {
+            rc = write_snapshot_which(c, 999998, 1, a);
+            if (v) std::printf("write z = 0.4 at step%d\n", tn + 1);
+            write_num++;
+        } else if (a > 0.5 && write_num == (c->p.stan ? 2 : 3)) {
+            rc = write_snapshot_which(c, 999997, 1, a);
+            if (v) std::printf("write z = 1 at step%d\n", tn + 1);
+            write_num++;
+            stop = true;
+        } else if (!c->p.stan && a > 0.333 && write_num == 2) {
+            rc = write_snapshot_which(c, 999996, 1, a);
+            if (v) std::printf("write z = 2 at step%d\n", tn + 1);
+            write_num++;
+        } else if (a > 0.25 && write_num == 2) {
+            rc = write_snapshot_which(c, write_sten_counter, 1, a);
+            if (v) std::printf("write z < 3  at step%d\n", write_sten_counter);
+            write_sten_counter++;
+        } else if (a > 0.25 && write_num == 1) {
+            rc = write_snapshot_which(c, 999995, 1, a);
+            if (v) std::printf("write z = 3 at step%d\n", tn + 1);
+            write_num++;
+        } else if (a > 0.105 && write_num == 0) {
+            rc = write_snapshot_which(c, 999994, 1, a);
+            if (v) std::printf("write z = 8.5 at step%d\n", tn + 1);
+            write_num++;
+        } else if ((tn % c->p.t_write == 0) || tn == c->p.t_stop - 1) {
+            rc = write_snapshot_which(c, tn + 1, 1, a);
+        }
+        if (rc) return rc;
+        if (stop) break;
+        if (v) std::printf("before write %d %g\n", write_num, 0.01 * write_num + 1);
+        if (v) std::printf(" tn = %d\n", tn);
+        CTX_STR(c, IFDM_ERR_CUDA, c->eng.passes_only());
+        if (v) {
+            CTX_CUDA(c, cudaStreamSynchronize(c->stream));
+            std::printf("simulation takes:0 seconds\n");
+            std::fflush(stdout);
+        }
+    }
+    CTX_CUDA(c, cudaStreamSynchronize(c->stream));
+    return IFDM_OK;
+}
+
+int ifdm_profile_passes(ifdm_ctx *c, int nsteps, double dt_scale, double *ms_out, const char **names_out, int cap) {
+    if (!c || nsteps <= 0) return IFDM_ERR_ARGS;
+    if (!c->have_psi) return fail(c, IFDM_ERR_STATE, "no wave function loaded");
+    std::vector<double> ms;
+    CTX_STR(c, IFDM_ERR_CUDA, c->eng.profile(nsteps, dt_scale, ms));
+    for (int i = 0; i < kNumPasses && i < cap; ++i) {
+        if (ms_out) ms_out[i] = ms[i];
+        if (names_out) names_out[i] = kPassNames[i];
+    }
+    return kNumPasses;
+}
+
+int ifdm_pass_bytes(ifdm_ctx *c, double *bytes_out, int cap) {
+    if (!c) return IFDM_ERR_ARGS;
+    auto b = c->eng.pass_bytes();
+    for (int i = 0; i < (int)b.size() && i < cap; ++i) bytes_out[i] = b[i];
+    return (int)b.size();
+}
+
+int ifdm_fft3d(void *data, int n, int precision, int sign, void *stream) {
+    if (!data || (sign != 1 && sign != -1)) return IFDM_ERR_ARGS;
+    if (!supported_n(n)) return IFDM_ERR_UNSUPPORTED;
+    std::string e = fft3d(data, n, precision, sign, (cudaStream_t)stream);
+    return e.empty() ? IFDM_OK : IFDM_ERR_CUDA;
+}
+
+}  // extern "C"

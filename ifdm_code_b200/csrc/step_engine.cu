@@ -1,0 +1,409 @@
+// step_engine.cu -- buffers, twiddle tables and launch sequence of the fused
+// leap-frog step (kernels in step_kernels.cuh / timestep.cuh).
+#include "physics.hpp"
+#include "step_engine.hpp"
+#include "timestep.cuh"
+
+#include <cmath>
+#include <cstdio>
+#include <cstring>
+
+namespace ifdm {
+
+const char *const kPassNames[kNumPasses] = {
+    "T_timestep", "P1_kick_fft_z", "P2_fft_y", "P3_fft_x_drift_ifft_x", "P4_ifft_y",
+    "P5_ifft_z_density_r2c_z", "P6_fft_y_half", "P7_fft_x_poisson_ifft_x", "P8_ifft_y_half", "P9_c2r_z_phi"};
+
+#define CUDA_TRY(expr)                                                                   \
+    do {                                                                                 \
+        cudaError_t e_ = (expr);                                                         \
+        if (e_ != cudaSuccess) return std::string(#expr) + ": " + cudaGetErrorString(e_); \
+    } while (0)
+
+bool supported_n(int n) {
+    switch (n) {
+        case 16: case 32: case 48: case 64: case 96: case 128: case 256: case 512: return true;
+        default: return false;
+    }
+}
+
+// ---------------------------------------------------------------- per-N ops --
+template <typename R, int N> struct Box {
+    using C = cx<R>;
+    using TL = Tile<R, N>;
+    static constexpr int NH = N / 2 + 1;
+    static constexpr int NHP = half_pitch<R>(N);
+    static constexpr size_t SM = TL::SMEM;
+    static constexpr size_t SM9 = size_t(N + 1) * TL::LP * sizeof(C);
+    // every launch covers its array exactly: no partial tiles
+    static_assert((N * N) % TL::L == 0, "z/y/x tiles must divide N^2 lines");
+    static_assert((N * NHP) % TL::L == 0, "half-spectrum tiles must divide N*NHP lines");
+    static_assert(NHP >= NH, "half-spectrum pitch");
+    static_assert(TL::NT <= 1024, "block size");
+    static_assert(SM9 <= 227 * 1024, "shared memory per block");
+
+    template <typename K> static cudaError_t prep(K kern, size_t smem) {
+        return cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    }
+
+    static std::string configure() {
+        static bool done = false;
+        if (done) return "";
+        CUDA_TRY(prep(k_kick_fft_z<R, N>, SM));
+        CUDA_TRY(prep(k_fft_yx<R, N, -1, 1>, SM));
+        CUDA_TRY(prep(k_fft_yx<R, N, +1, 1>, SM));
+        CUDA_TRY(prep(k_fft_yx<R, N, -1, 2>, SM));
+        CUDA_TRY(prep(k_fft_yx<R, N, +1, 2>, SM));
+        CUDA_TRY(prep(k_fft_x_drift<R, N>, SM));
+        CUDA_TRY(prep(k_density_r2c_z<R, N, true>, SM));
+        CUDA_TRY(prep(k_density_r2c_z<R, N, false>, SM));
+        CUDA_TRY(prep(k_fft_x_poisson<R, N>, SM));
+        CUDA_TRY(prep(k_c2r_z_phi<R, N>, SM9));
+        CUDA_TRY(prep(k_fft_z<R, N, -1>, SM));
+        CUDA_TRY(prep(k_fft_z<R, N, +1>, SM));
+        done = true;
+        return "";
+    }
+
+    static unsigned zblocks() { return unsigned(size_t(N) * N / TL::L); }
+    static unsigned hblocks() { return unsigned(size_t(N) * NHP / TL::L); }
+
+    // one pass by index 1..9
+    static void pass(int p, cudaStream_t s, C *psi, R *phi, C *rhok, TState *ts, const C *drift, const C *tw,
+                     const C *twh, double mu, long wr, int wt) {
+        const unsigned nt = TL::NT;
+        switch (p) {
+            case 1: k_kick_fft_z<R, N><<<zblocks(), nt, SM, s>>>(psi, phi, ts, tw); break;
+            case 2: k_fft_yx<R, N, -1, 1><<<zblocks(), nt, SM, s>>>(psi, N, N, tw); break;
+            case 3: k_fft_x_drift<R, N><<<zblocks(), nt, SM, s>>>(psi, drift, tw); break;
+            case 4: k_fft_yx<R, N, +1, 1><<<zblocks(), nt, SM, s>>>(psi, N, N, tw); break;
+            case 5: k_density_r2c_z<R, N, true><<<zblocks(), nt, SM, s>>>(psi, rhok, ts, mu, tw, twh); break;
+            case 6: k_fft_yx<R, N, -1, 1><<<hblocks(), nt, SM, s>>>(rhok, NHP, NH, tw); break;
+            case 7: k_fft_x_poisson<R, N><<<hblocks(), nt, SM, s>>>(rhok, tw); break;
+            case 8: k_fft_yx<R, N, +1, 1><<<hblocks(), nt, SM, s>>>(rhok, NHP, NH, tw); break;
+            case 9: k_c2r_z_phi<R, N><<<zblocks(), nt, SM9, s>>>(rhok, phi, ts, wr, wt, tw, twh); break;
+            default: break;
+        }
+    }
+
+    static void initial_density(cudaStream_t s, C *psi, C *rhok, TState *ts, const C *tw, const C *twh,
+                                double mu) {
+        k_density_r2c_z<R, N, false><<<zblocks(), TL::NT, SM, s>>>(psi, rhok, ts, mu, tw, twh);
+    }
+
+    static void fft3d(C *data, int sign, const C *tw, cudaStream_t s) {
+        const unsigned nt = TL::NT;
+        if (sign < 0) {
+            k_fft_z<R, N, -1><<<zblocks(), nt, SM, s>>>(data, tw);
+            k_fft_yx<R, N, -1, 1><<<zblocks(), nt, SM, s>>>(data, N, N, tw);
+            k_fft_yx<R, N, -1, 2><<<zblocks(), nt, SM, s>>>(data, N, N, tw);
+        } else {
+            k_fft_z<R, N, +1><<<zblocks(), nt, SM, s>>>(data, tw);
+            k_fft_yx<R, N, +1, 1><<<zblocks(), nt, SM, s>>>(data, N, N, tw);
+            k_fft_yx<R, N, +1, 2><<<zblocks(), nt, SM, s>>>(data, N, N, tw);
+        }
+    }
+};
+
+// Runtime N -> Box<R, N>
+template <typename R, typename F> static std::string with_box(int n, F &&f) {
+    switch (n) {
+        case 16: return f(Box<R, 16>{});
+        case 32: return f(Box<R, 32>{});
+        case 48: return f(Box<R, 48>{});
+        case 64: return f(Box<R, 64>{});
+        case 96: return f(Box<R, 96>{});
+        case 128: return f(Box<R, 128>{});
+        case 256: return f(Box<R, 256>{});
+        case 512: return f(Box<R, 512>{});
+        default: return "unsupported grid size " + std::to_string(n);
+    }
+}
+template <typename F> static std::string with_box2(int n, int prec, F &&f) {
+    return prec == 0 ? with_box<double>(n, f) : with_box<float>(n, f);
+}
+
+// twiddles exp(-2 pi i m / n), m < n, from long double
+template <typename C> static std::vector<C> twiddles(int n) {
+    std::vector<C> t(n);
+    const long double twopi = 6.283185307179586476925286766559005768L;
+    for (int m = 0; m < n; ++m) {
+        const long double ang = -twopi * (long double)m / (long double)n;
+        t[m].x = (decltype(t[m].x))cosl(ang);
+        t[m].y = (decltype(t[m].y))sinl(ang);
+    }
+    return t;
+}
+
+// cached per-(n, precision) tables on the current device
+static std::string get_twiddles(int n, int prec, void **out) {
+    struct Entry { int dev, n, prec; void *p; };
+    static std::vector<Entry> cache;
+    int dev = 0;
+    CUDA_TRY(cudaGetDevice(&dev));
+    for (auto &e : cache)
+        if (e.dev == dev && e.n == n && e.prec == prec) { *out = e.p; return ""; }
+    void *p = nullptr;
+    if (prec == 0) {
+        auto t = twiddles<double2>(n);
+        CUDA_TRY(cudaMalloc(&p, sizeof(double2) * n));
+        CUDA_TRY(cudaMemcpy(p, t.data(), sizeof(double2) * n, cudaMemcpyHostToDevice));
+    } else {
+        auto t = twiddles<float2>(n);
+        CUDA_TRY(cudaMalloc(&p, sizeof(float2) * n));
+        CUDA_TRY(cudaMemcpy(p, t.data(), sizeof(float2) * n, cudaMemcpyHostToDevice));
+    }
+    cache.push_back({dev, n, prec, p});
+    *out = p;
+    return "";
+}
+
+// ------------------------------------------------------------ StepEngine --
+StepEngine::~StepEngine() {
+    cudaFree(psi_);
+    cudaFree(phi_);
+    cudaFree(rhok_);
+    cudaFree(drift64_);
+    cudaFree(drift32_);
+    cudaFree(ts_);
+}
+
+std::string StepEngine::init(const EngineConfig &cfg, cudaStream_t stream) {
+    cfg_ = cfg;
+    stream_ = stream;
+    const int N = cfg.N;
+    if (!supported_n(N)) return "unsupported grid size " + std::to_string(N);
+    const size_t n3 = n3_();
+    const size_t cs = cfg.precision == 0 ? 16 : 8, rs = cs / 2;
+    const int nhp = cfg.precision == 0 ? half_pitch<double>(N) : half_pitch<float>(N);
+    CUDA_TRY(cudaMalloc(&psi_, n3 * cs));
+    CUDA_TRY(cudaMalloc(&phi_, n3 * rs));
+    CUDA_TRY(cudaMalloc(&rhok_, size_t(N) * N * nhp * cs));
+    CUDA_TRY(cudaMemsetAsync(rhok_, 0, size_t(N) * N * nhp * cs, stream_));
+    CUDA_TRY(cudaMalloc(&drift64_, sizeof(double2) * N));
+    CUDA_TRY(cudaMalloc(&drift32_, sizeof(float2) * N));
+    CUDA_TRY(cudaMalloc(&ts_, sizeof(TState)));
+    CUDA_TRY(cudaMemsetAsync(ts_, 0, sizeof(TState), stream_));
+    std::string e = get_twiddles(N, cfg.precision, &tw_);
+    if (!e.empty()) return e;
+    e = get_twiddles(N / 2, cfg.precision, &twh_);
+    if (!e.empty()) return e;
+    e = with_box2(N, cfg.precision, [](auto box) { return decltype(box)::configure(); });
+    if (!e.empty()) return e;
+    // max|phi| scan window of the reference: first N^3 doubles of the padded
+    // [N][N][2(N/2+1)] array (the vector holds only N^3 elements,
+    // src/struct3D.h:110,117; scanned at src/CosmoBEC_MPI.cpp:26)
+    const long P = 2 * (N / 2 + 1);
+    const long tot = long(N) * N * N;
+    win_rows_ = tot / P;
+    win_tail_ = int(tot - win_rows_ * P);
+    return "";
+}
+
+size_t StepEngine::n3_() const { return size_t(cfg_.N) * cfg_.N * cfg_.N; }
+
+std::string StepEngine::set_physics(double a, double rhoc) {
+    using namespace phys;
+    cfg_.rhoc = rhoc;
+    const double m = cfg_.mfdm, ms = cfg_.mfdm_solar;
+    const double S2 = rhoc / ms;
+    S_ = std::sqrt(S2);
+    mu_ = 1.0;
+    Phi0_ = 4.0 * M_PI * bigG * rhoc * (cfg_.xmax / M_PI) * (cfg_.xmax / M_PI);
+    Phys &ph = phys_;
+    ph.A_KE = 4. / (3. * M_PI) * (m / pow(c, 2)) / hbar * pow(cfg_.dx, 2);
+    ph.B_PE = 2. * M_PI * hbar / (m / pow(c, 2));
+    ph.C_QI = cfg_.g != 0 ? 2. * M_PI * hbar / fabs(cfg_.g) : 0.0;
+    ph.g = cfg_.g;
+    ph.H0 = H_0;
+    ph.Om = Omega_m0;
+    ph.kP = m / pow(c, 2) / hbar * Phi0_;
+    ph.kQ = cfg_.g / hbar * S2;
+    ph.kin = 0.5 * hbar / (m / pow(c, 2)) * (M_PI / cfg_.xmax) * (M_PI / cfg_.xmax);
+    ph.Phi0 = Phi0_;
+    ph.S2 = S2;
+    ph.dt_scale = 1.0;
+    ph.N = cfg_.N;
+    ph.limit = 64;
+    TState t;
+    std::memset(&t, 0, sizeof t);
+    t.a = a;
+    CUDA_TRY(cudaMemcpyAsync(ts_, &t, sizeof t, cudaMemcpyHostToDevice, stream_));
+    CUDA_TRY(cudaStreamSynchronize(stream_));
+    return "";
+}
+
+std::string StepEngine::load_psi(const double *psi, bool on_device, double a, double rhoc) {
+    std::string e = set_physics(a, rhoc);
+    if (!e.empty()) return e;
+    const size_t n3 = n3_();
+    const double invS = 1.0 / S_;
+    const int prec = cfg_.precision;
+    if (on_device) {
+        if (prec == 0) k_psi_in<double><<<1184, 256, 0, stream_>>>((const double2 *)psi, (double2 *)psi_, invS, n3);
+        else k_psi_in<float><<<1184, 256, 0, stream_>>>((const double2 *)psi, (float2 *)psi_, invS, n3);
+        CUDA_TRY(cudaGetLastError());
+    } else {
+        const size_t chunk = std::min<size_t>(n3, size_t(1) << 22);
+        double2 *stage = nullptr;
+        CUDA_TRY(cudaMalloc(&stage, chunk * sizeof(double2)));
+        for (size_t off = 0; off < n3; off += chunk) {
+            const size_t cnt = std::min(chunk, n3 - off);
+            CUDA_TRY(cudaMemcpyAsync(stage, psi + 2 * off, cnt * sizeof(double2), cudaMemcpyHostToDevice, stream_));
+            if (prec == 0)
+                k_psi_in<double><<<1184, 256, 0, stream_>>>(stage, (double2 *)psi_ + off, invS, cnt);
+            else
+                k_psi_in<float><<<1184, 256, 0, stream_>>>(stage, (float2 *)psi_ + off, invS, cnt);
+            CUDA_TRY(cudaGetLastError());
+        }
+        CUDA_TRY(cudaStreamSynchronize(stream_));
+        cudaFree(stage);
+    }
+    return launch_initial_density();
+}
+
+std::string StepEngine::launch_initial_density() {
+    const double mu = mu_;
+    return with_box2(cfg_.N, cfg_.precision, [&](auto box) -> std::string {
+        using B = decltype(box);
+        using C = typename B::C;
+        using R = decltype(C{}.x);
+        C *psi = (C *)psi_, *rhok = (C *)rhok_;
+        R *phi = (R *)phi_;
+        const C *tw = (const C *)tw_, *twh = (const C *)twh_;
+        B::initial_density(stream_, psi, rhok, ts_, tw, twh, mu);
+        for (int p = 6; p <= 9; ++p) B::pass(p, stream_, psi, phi, rhok, ts_, nullptr, tw, twh, mu, win_rows_, win_tail_);
+        CUDA_TRY(cudaGetLastError());
+        return "";
+    });
+}
+
+std::string StepEngine::launch_timestep(double dt_scale) {
+    Phys ph = phys_;
+    ph.dt_scale = dt_scale;
+    const int nt = cfg_.N < 32 ? 32 : (cfg_.N > 512 ? 512 : cfg_.N);
+    k_timestep<<<1, nt, 0, stream_>>>(ts_, ph, drift64_, drift32_);
+    CUDA_TRY(cudaGetLastError());
+    return "";
+}
+
+std::string StepEngine::launch_passes(cudaEvent_t *ev) {
+    const double mu = mu_;
+    return with_box2(cfg_.N, cfg_.precision, [&](auto box) -> std::string {
+        using B = decltype(box);
+        using C = typename B::C;
+        using R = decltype(C{}.x);
+        C *psi = (C *)psi_, *rhok = (C *)rhok_;
+        R *phi = (R *)phi_;
+        const C *tw = (const C *)tw_, *twh = (const C *)twh_;
+        const C *drift = cfg_.precision == 0 ? (const C *)(void *)drift64_ : (const C *)(void *)drift32_;
+        for (int p = 1; p <= 9; ++p) {
+            B::pass(p, stream_, psi, phi, rhok, ts_, drift, tw, twh, mu, win_rows_, win_tail_);
+            if (ev) CUDA_TRY(cudaEventRecord(ev[p], stream_));
+        }
+        CUDA_TRY(cudaGetLastError());
+        return "";
+    });
+}
+
+std::string StepEngine::timestep_only(double dt_scale) { return launch_timestep(dt_scale); }
+std::string StepEngine::passes_only() { return launch_passes(nullptr); }
+
+std::string StepEngine::step(int nsteps, double dt_scale) {
+    for (int i = 0; i < nsteps; ++i) {
+        std::string e = launch_timestep(dt_scale);
+        if (!e.empty()) return e;
+        e = launch_passes(nullptr);
+        if (!e.empty()) return e;
+    }
+    return "";
+}
+
+std::string StepEngine::profile(int nsteps, double dt_scale, std::vector<double> &ms) {
+    cudaEvent_t ev[kNumPasses + 1];
+    for (auto &e : ev) CUDA_TRY(cudaEventCreate(&e));
+    ms.assign(kNumPasses, 0.0);
+    for (int i = 0; i < nsteps; ++i) {
+        CUDA_TRY(cudaEventRecord(ev[0], stream_));
+        std::string e = launch_timestep(dt_scale);
+        if (!e.empty()) return e;
+        CUDA_TRY(cudaEventRecord(ev[1], stream_));
+        // passes record ev[p] after pass p; shift so ev[p+1] follows pass p
+        cudaEvent_t pe[kNumPasses];
+        for (int p = 1; p <= 9; ++p) pe[p] = ev[p + 1];
+        e = launch_passes(pe);
+        if (!e.empty()) return e;
+        CUDA_TRY(cudaEventSynchronize(ev[kNumPasses]));
+        for (int p = 0; p < kNumPasses; ++p) {
+            float t = 0.f;
+            CUDA_TRY(cudaEventElapsedTime(&t, ev[p], ev[p + 1]));
+            ms[p] += t;
+        }
+    }
+    for (auto &v : ms) v /= nsteps;
+    for (auto &e : ev) cudaEventDestroy(e);
+    return "";
+}
+
+std::vector<double> StepEngine::pass_bytes() const {
+    const double n3 = (double)n3_();
+    const double N = cfg_.N;
+    const double nh = N * N * (N / 2 + 1);
+    const double cs = cfg_.precision == 0 ? 16 : 8, rs = cs / 2;
+    return {0.0,
+            n3 * (2 * cs + rs),         // P1 psi in/out + phi in
+            2 * cs * n3,                // P2
+            2 * cs * n3,                // P3
+            2 * cs * n3,                // P4
+            2 * cs * n3 + cs * nh,      // P5 psi in/out + half spectrum out
+            2 * cs * nh,                // P6
+            2 * cs * nh,                // P7
+            2 * cs * nh,                // P8
+            cs * nh + rs * n3};         // P9 half spectrum in + phi out
+}
+
+std::string StepEngine::psi_out(double *dev_out, int which) {
+    const size_t n3 = n3_();
+    if (cfg_.precision == 0)
+        k_psi_out<double><<<1184, 256, 0, stream_>>>((const double2 *)psi_, (const double *)phi_, ts_, which, S_,
+                                                     (double2 *)dev_out, n3);
+    else
+        k_psi_out<float><<<1184, 256, 0, stream_>>>((const float2 *)psi_, (const float *)phi_, ts_, which, S_,
+                                                    (double2 *)dev_out, n3);
+    CUDA_TRY(cudaGetLastError());
+    return "";
+}
+
+std::string StepEngine::phi_out(double *dev_out) {
+    const size_t n3 = n3_();
+    if (cfg_.precision == 0)
+        k_phi_out<double><<<1184, 256, 0, stream_>>>((const double *)phi_, Phi0_, dev_out, n3);
+    else
+        k_phi_out<float><<<1184, 256, 0, stream_>>>((const float *)phi_, Phi0_, dev_out, n3);
+    CUDA_TRY(cudaGetLastError());
+    return "";
+}
+
+std::string StepEngine::read_state(TState &out) {
+    CUDA_TRY(cudaMemcpyAsync(&out, ts_, sizeof(TState), cudaMemcpyDeviceToHost, stream_));
+    CUDA_TRY(cudaStreamSynchronize(stream_));
+    return "";
+}
+
+std::string fft3d(void *data, int n, int precision, int sign, cudaStream_t stream) {
+    if (!supported_n(n)) return "unsupported grid size " + std::to_string(n);
+    void *tw = nullptr;
+    std::string e = get_twiddles(n, precision, &tw);
+    if (!e.empty()) return e;
+    return with_box2(n, precision, [&](auto box) -> std::string {
+        using B = decltype(box);
+        using C = typename B::C;
+        std::string e2 = B::configure();
+        if (!e2.empty()) return e2;
+        B::fft3d((C *)data, sign, (const C *)tw, stream);
+        CUDA_TRY(cudaGetLastError());
+        return "";
+    });
+}
+
+}  // namespace ifdm

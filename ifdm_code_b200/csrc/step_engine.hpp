@@ -1,0 +1,85 @@
+// step_engine.hpp -- device state and pass launcher of one simulation box.
+#pragma once
+
+#include <cuda_runtime.h>
+
+#include "state_types.hpp"
+
+#include <string>
+#include <vector>
+
+namespace ifdm {
+
+struct EngineConfig {
+    int N = 0;
+    int precision = 0;  // 0 FP64, 1 FP32
+    // physics (natural units of the reference)
+    double mfdm = 0, g = 0, xmax = 0, dx = 0;
+    double mfdm_solar = 0, rhoc = 0;
+    double dt_scale = 1.0;
+};
+
+// Names of the fused passes in launch order (timestep first).
+constexpr int kNumPasses = 10;
+extern const char *const kPassNames[kNumPasses];
+
+class StepEngine {
+  public:
+    StepEngine() = default;
+    ~StepEngine();
+    StepEngine(const StepEngine &) = delete;
+    StepEngine &operator=(const StepEngine &) = delete;
+
+    // Allocates device buffers on the current device; returns "" or an error.
+    std::string init(const EngineConfig &cfg, cudaStream_t stream);
+    // psi (host or device complex128, N^3) -> scaled state; sets a and rho_c,
+    // runs the initial density/Poisson passes.  Asynchronous.
+    std::string load_psi(const double *psi_c128, bool on_device, double a, double rhoc);
+    // nsteps fixed-mode steps (timestep + 9 passes each).  Asynchronous.
+    std::string step(int nsteps, double dt_scale);
+    // Per-pass event timing of nsteps steps (synchronous); ms per step.
+    std::string profile(int nsteps, double dt_scale, std::vector<double> &ms);
+    // Algorithmic HBM bytes per pass per step.
+    std::vector<double> pass_bytes() const;
+    // psi as complex128 into dev_out (device), which: 0 raw, 1 snapshot kick, 2 pending kick.
+    std::string psi_out(double *dev_out, int which);
+    std::string phi_out(double *dev_out);
+    // copy the TState to host (synchronous)
+    std::string read_state(TState &out);
+    // one step split for the native loop: timestep only / passes only
+    std::string timestep_only(double dt_scale);
+    std::string passes_only();
+
+    int N() const { return cfg_.N; }
+    int precision() const { return cfg_.precision; }
+    cudaStream_t stream() const { return stream_; }
+    double S() const { return S_; }
+    double Phi0() const { return Phi0_; }
+    size_t n3() const { return size_t(cfg_.N) * cfg_.N * cfg_.N; }
+    void *psi_ptr() const { return psi_; }
+
+  private:
+    std::string launch_timestep(double dt_scale);
+    std::string launch_passes(cudaEvent_t *ev);  // ev: optional 10 events (after each pass)
+    std::string launch_initial_density();
+    std::string set_physics(double a, double rhoc);
+    size_t n3_() const;
+
+    EngineConfig cfg_{};
+    cudaStream_t stream_ = nullptr;
+    void *psi_ = nullptr, *phi_ = nullptr, *rhok_ = nullptr;
+    void *tw_ = nullptr, *twh_ = nullptr;  // precision-typed twiddle tables (N and N/2)
+    double2 *drift64_ = nullptr;
+    float2 *drift32_ = nullptr;
+    TState *ts_ = nullptr;
+    Phys phys_{};
+    double S_ = 1, Phi0_ = 1, mu_ = 1;
+    long win_rows_ = 0;
+    int win_tail_ = 0;
+};
+
+// Plain in-place 3-D c2c FFT of device data (complex128 if precision 0).
+std::string fft3d(void *data, int n, int precision, int sign, cudaStream_t stream);
+bool supported_n(int n);
+
+}  // namespace ifdm

@@ -1,0 +1,350 @@
+// step_kernels.cuh -- the fused passes of one leap-frog step (sm_100a).
+//
+// One step of the reference (src/CosmoBEC_MPI.cpp:218-219 then :121-159) is
+//   poisson; timestep; kick/2; FFT; drift; iFFT; poisson; kick/2
+// Here the two half kicks that meet between consecutive steps are merged
+// (same phi, same |psi| -- the kick only rotates phases), the Poisson solve
+// before the timestep reuses the one at the end of the previous step, and
+// every elementwise operation rides inside an FFT axis pass.  Per step:
+//
+//   T  timestep   device quadrature, merged kick coefficients, drift tables
+//   P1 z-pass     load psi + phi, kick, forward FFT along z
+//   P2 y-pass     forward FFT along y
+//   P3 x-pass     forward FFT along x, drift, inverse FFT along x
+//   P4 y-pass     inverse FFT along y
+//   P5 z-pass     inverse FFT along z -> psi; rho = |psi|^2 - mu; max|psi|^2;
+//                 real-to-half-complex FFT of rho along z
+//   P6 y-pass     forward FFT along y (half spectrum)
+//   P7 x-pass     forward FFT along x, phi_k = -rho_k / kappa^2, inverse FFT
+//   P8 y-pass     inverse FFT along y (half spectrum)
+//   P9 z-pass     half-complex-to-real FFT along z, /N^3 -> phi; max|phi|
+//
+// Units: psi is stored as psi/S with S^2 = rho_c / m_solar, so |psi_s|^2 is
+// the density in units of the mean (this keeps FP32 in range: |psi| ~ 1e50
+// in the reference's units).  phi is stored as phi/Phi0 with
+// Phi0 = 4 pi G m_solar S^2 (xmax/pi)^2, so the Poisson multiplier is
+// -1/kappa^2 with integer kappa.  All scale factors are FP64 and folded into
+// the coefficients the timestep kernel writes.
+#pragma once
+
+#include "fft_engine.cuh"
+#include "state_types.hpp"
+
+namespace ifdm {
+
+// ------------------------------------------------------------ tile config --
+template <typename R, int N> struct Tile {
+    static constexpr int E = Plan<N>::E;
+    static constexpr int T = N / E;                              // threads per line
+    static constexpr int PH = sizeof(cx<R>) == 16 ? 8 : 16;      // threads per smem phase
+    static constexpr int LW = (256 / T > PH) ? 256 / T : PH;     // lines per tile
+    static constexpr int L = LW;
+    static constexpr int LP = L + 1;
+    static constexpr int NT = L * T;                             // threads per block
+    static constexpr size_t SMEM = size_t(N) * LP * sizeof(cx<R>);
+};
+
+// Half-spectrum row pitch: N/2+1 rounded up so rows start on 128-byte lines.
+template <typename R> __host__ __device__ constexpr int half_pitch(int n) {
+    return sizeof(R) == 8 ? ((n / 2 + 1 + 7) / 8) * 8 : ((n / 2 + 1 + 15) / 16) * 16;
+}
+
+__host__ __device__ constexpr int kappa(int i, int n) { return i < n / 2 ? i : i - n; }
+
+__device__ __forceinline__ void atomic_max_nonneg(unsigned long long *addr, double v) {
+    // non-negative IEEE doubles order like their bit patterns
+    atomicMax(addr, (unsigned long long)__double_as_longlong(v));
+}
+
+template <typename R> __device__ __forceinline__ R warp_max(R v) {
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) v = fmax(v, __shfl_xor_sync(0xffffffffu, v, o));
+    return v;
+}
+
+// exp(-i p) for the kick; FP32 reduces the FP64 argument mod 2 pi first.
+template <typename R> __device__ __forceinline__ cx<R> expmi(double p);
+template <> __device__ __forceinline__ double2 expmi<double>(double p) {
+    double s, c;
+    sincos(p, &s, &c);
+    return mkc(c, -s);
+}
+template <> __device__ __forceinline__ float2 expmi<float>(double p) {
+    const double twopi = 6.283185307179586476925286766559;
+    const double pr = p - twopi * rint(p * (1.0 / twopi));
+    float s, c;
+    sincosf((float)pr, &s, &c);
+    return mkc(c, -s);
+}
+
+// ------------------------------------------------------------- z-passes ---
+// Tiles of L consecutive rows (row r = x*N + y), row pitch N, contiguous.
+
+template <typename R, int N, int DIR>
+__global__ void __launch_bounds__(Tile<R, N>::NT) k_fft_z(cx<R> *__restrict__ data, const cx<R> *__restrict__ tw) {
+    using C = cx<R>;
+    using TL = Tile<R, N>;
+    extern __shared__ __align__(16) unsigned char smraw[];
+    C *sm = reinterpret_cast<C *>(smraw);
+    const size_t base = size_t(blockIdx.x) * TL::L * N;
+    for (int f = threadIdx.x; f < TL::L * N; f += TL::NT) sm[(f % N) * TL::LP + f / N] = data[base + f];
+    __syncthreads();
+    fft_tile<C, N, DIR, TL::L, TL::LP>(sm, tw);
+    for (int f = threadIdx.x; f < TL::L * N; f += TL::NT) data[base + f] = sm[(f % N) * TL::LP + f / N];
+}
+
+// P1: kick with the merged coefficients, then forward FFT along z.
+template <typename R, int N>
+__global__ void __launch_bounds__(Tile<R, N>::NT)
+    k_kick_fft_z(cx<R> *__restrict__ psi, const R *__restrict__ phi, const TState *__restrict__ ts,
+                 const cx<R> *__restrict__ tw) {
+    using C = cx<R>;
+    using TL = Tile<R, N>;
+    extern __shared__ __align__(16) unsigned char smraw[];
+    C *sm = reinterpret_cast<C *>(smraw);
+    const double cp = ts->coefP, cq = ts->coefQ;
+    const size_t base = size_t(blockIdx.x) * TL::L * N;
+    for (int f = threadIdx.x; f < TL::L * N; f += TL::NT) {
+        C v = psi[base + f];
+        const double p = cp * (double)phi[base + f] + cq * (double)cnorm2(v);
+        sm[(f % N) * TL::LP + f / N] = cmul(v, expmi<R>(p));
+    }
+    __syncthreads();
+    fft_tile<C, N, -1, TL::L, TL::LP>(sm, tw);
+    for (int f = threadIdx.x; f < TL::L * N; f += TL::NT) psi[base + f] = sm[(f % N) * TL::LP + f / N];
+}
+
+// P5 (DO_IFFT) / initial density (no IFFT): rho = |psi|^2 - mu, max |psi|^2,
+// real-to-half-complex FFT of rho along z into rhok (pitch NHP).
+template <typename R, int N, bool DO_IFFT>
+__global__ void __launch_bounds__(Tile<R, N>::NT)
+    k_density_r2c_z(cx<R> *__restrict__ psi, cx<R> *__restrict__ rhok, TState *__restrict__ ts, double mu,
+                    const cx<R> *__restrict__ tw, const cx<R> *__restrict__ twh) {
+    using C = cx<R>;
+    using TL = Tile<R, N>;
+    constexpr int NH = N / 2 + 1;
+    constexpr int NHP = half_pitch<R>(N);
+    constexpr int M = N / 2;
+    extern __shared__ __align__(16) unsigned char smraw[];
+    C *sm = reinterpret_cast<C *>(smraw);
+    const size_t row0 = size_t(blockIdx.x) * TL::L;
+    const size_t base = row0 * N;
+    if (DO_IFFT) {
+        for (int f = threadIdx.x; f < TL::L * N; f += TL::NT) sm[(f % N) * TL::LP + f / N] = psi[base + f];
+        __syncthreads();
+        fft_tile<C, N, +1, TL::L, TL::LP>(sm, tw);
+    }
+    // rho values: thread keeps its E elements (fixed stride NT over the tile)
+    R rho[TL::E];
+    double mx = 0.0;
+#pragma unroll
+    for (int i = 0; i < TL::E; ++i) {
+        const int f = threadIdx.x + i * TL::NT;
+        C v;
+        if (DO_IFFT) {
+            v = sm[(f % N) * TL::LP + f / N];
+            psi[base + f] = v;
+        } else {
+            v = psi[base + f];
+        }
+        const double n2 = (double)cnorm2(v);
+        mx = fmax(mx, n2);
+        rho[i] = (R)(n2 - mu);
+    }
+    mx = warp_max(mx);
+    if ((threadIdx.x & 31) == 0) atomic_max_nonneg(&ts->maxrho_bits, mx);
+    __syncthreads();
+    // pack z_m = rho_{2m} + i rho_{2m+1} into the half tile (rows m < N/2)
+    R *smr = reinterpret_cast<R *>(sm);
+#pragma unroll
+    for (int i = 0; i < TL::E; ++i) {
+        const int f = threadIdx.x + i * TL::NT;
+        const int l = f / N, n = f % N;
+        smr[2 * ((n >> 1) * TL::LP + l) + (n & 1)] = rho[i];
+    }
+    __syncthreads();
+    fft_tile<C, M, -1, TL::L, TL::LP>(sm, twh);
+    // X_k = (Z_k + conj Z_{M-k})/2 - i w^k (Z_k - conj Z_{M-k})/2, k = 0..M
+    for (int f = threadIdx.x; f < TL::L * NH; f += TL::NT) {
+        const int l = f / NH, k = f % NH;
+        const C zk = sm[(k % M) * TL::LP + l];
+        const C zc = cconj(sm[((M - k) % M) * TL::LP + l]);
+        const C e = cscale(zk + zc, R(0.5));
+        const C o = cscale(zk - zc, R(0.5));
+        const C w = __ldg(tw + (k % N));
+        // -i * w * o
+        const C wo = cmul(w, o);
+        rhok[(row0 + l) * NHP + k] = mkc(e.x + wo.y, e.y - wo.x);
+    }
+}
+
+// P9: half-complex-to-real FFT along z, scale by 1/N^3, store phi, max|phi|
+// over the reference's scan window (rows below win_rows, plus win_tail
+// elements of row win_rows; see the timestep kernel).
+template <typename R, int N>
+__global__ void __launch_bounds__(Tile<R, N>::NT)
+    k_c2r_z_phi(const cx<R> *__restrict__ rhok, R *__restrict__ phi, TState *__restrict__ ts, long win_rows,
+                int win_tail, const cx<R> *__restrict__ tw, const cx<R> *__restrict__ twh) {
+    using C = cx<R>;
+    using TL = Tile<R, N>;
+    constexpr int NHP = half_pitch<R>(N);
+    constexpr int M = N / 2;
+    extern __shared__ __align__(16) unsigned char smraw[];
+    C *sm = reinterpret_cast<C *>(smraw);
+    C *xs = sm + M * TL::LP;  // X_k rows k = 0..M staged after the Z tile
+    const size_t row0 = size_t(blockIdx.x) * TL::L;
+    for (int f = threadIdx.x; f < TL::L * (M + 1); f += TL::NT) {
+        const int l = f / (M + 1), k = f % (M + 1);
+        C x = rhok[(row0 + l) * NHP + k];
+        if (k == 0 || k == M) x.y = R(0);  // c2r ignores these imaginary parts
+        xs[k * TL::LP + l] = x;
+    }
+    __syncthreads();
+    // Z'_k = (X_k + conj X_{M-k}) + i conj(w^k) (X_k - conj X_{M-k}), k < M
+    for (int f = threadIdx.x; f < TL::L * M; f += TL::NT) {
+        const int l = f % TL::L, k = f / TL::L;
+        const C xk = xs[k * TL::LP + l];
+        const C xc = cconj(xs[(M - k) * TL::LP + l]);
+        const C e = xk + xc;
+        const C d = cmul(cconj(__ldg(tw + k)), xk - xc);
+        sm[k * TL::LP + l] = mkc(e.x - d.y, e.y + d.x);
+    }
+    __syncthreads();
+    fft_tile<C, M, +1, TL::L, TL::LP>(sm, twh);
+    const R *smr = reinterpret_cast<const R *>(sm);
+    const R inv = R(1.0 / ((double)N * N * N));
+    double mx = 0.0;
+    for (int f = threadIdx.x; f < TL::L * N; f += TL::NT) {
+        const int l = f / N, n = f % N;
+        const R v = smr[2 * ((n >> 1) * TL::LP + l) + (n & 1)] * inv;
+        phi[row0 * N + f] = v;
+        const long row = (long)(row0 + l);
+        if (row < win_rows || (row == win_rows && n < win_tail)) mx = fmax(mx, (double)fabs(v));
+    }
+    mx = warp_max(mx);
+    if ((threadIdx.x & 31) == 0) atomic_max_nonneg(&ts->maxphi_bits, mx);
+}
+
+// --------------------------------------------------------- y / x passes ---
+// AXIS 1 (y): line g -> (x, z) = (g / W, g % W), element n at (x*N + n)*W + z.
+// AXIS 2 (x): line g = column q, element n at n*N*W + q.
+// Lines with (g % W) >= VW are padding: loads and stores skipped.
+template <int AXIS> __device__ __forceinline__ size_t line_base(long g, int N, int W) {
+    return AXIS == 1 ? size_t(g / W) * N * W + (g % W) : size_t(g);
+}
+
+template <typename R, int N, int DIR, int AXIS>
+__global__ void __launch_bounds__(Tile<R, N>::NT)
+    k_fft_yx(cx<R> *__restrict__ data, int W, int VW, const cx<R> *__restrict__ tw) {
+    using C = cx<R>;
+    using TL = Tile<R, N>;
+    extern __shared__ __align__(16) unsigned char smraw[];
+    C *sm = reinterpret_cast<C *>(smraw);
+    const int l = threadIdx.x % TL::L;
+    const long g = long(blockIdx.x) * TL::L + l;
+    const bool valid = (g % W) < VW;
+    const size_t b = line_base<AXIS>(g, N, W);
+    const size_t S = AXIS == 1 ? size_t(W) : size_t(N) * W;
+    for (int n = threadIdx.x / TL::L; n < N; n += TL::NT / TL::L)
+        sm[n * TL::LP + l] = valid ? data[b + n * S] : mkc(R(0), R(0));
+    __syncthreads();
+    fft_tile<C, N, DIR, TL::L, TL::LP>(sm, tw);
+    if (valid)
+        for (int n = threadIdx.x / TL::L; n < N; n += TL::NT / TL::L) data[b + n * S] = sm[n * TL::LP + l];
+}
+
+// P3: x-pass forward, drift exp(-i s kappa^2) / N^3 from separable tables,
+// x-pass inverse.  drift[i] = exp(-i s kappa_i^2) written by the timestep.
+template <typename R, int N>
+__global__ void __launch_bounds__(Tile<R, N>::NT)
+    k_fft_x_drift(cx<R> *__restrict__ psi, const cx<R> *__restrict__ drift, const cx<R> *__restrict__ tw) {
+    using C = cx<R>;
+    using TL = Tile<R, N>;
+    extern __shared__ __align__(16) unsigned char smraw[];
+    C *sm = reinterpret_cast<C *>(smraw);
+    const int l = threadIdx.x % TL::L;
+    const long q = long(blockIdx.x) * TL::L + l;  // column = y*N + z
+    const size_t S = size_t(N) * N;
+    for (int n = threadIdx.x / TL::L; n < N; n += TL::NT / TL::L) sm[n * TL::LP + l] = psi[q + n * S];
+    __syncthreads();
+    fft_tile<C, N, -1, TL::L, TL::LP>(sm, tw);
+    const int y = int(q / N), z = int(q % N);
+    const C lf = cscale(cmul(__ldg(drift + y), __ldg(drift + z)), R(1.0 / ((double)N * N * N)));
+    for (int n = threadIdx.x / TL::L; n < N; n += TL::NT / TL::L)
+        sm[n * TL::LP + l] = cmul(sm[n * TL::LP + l], cmul(lf, __ldg(drift + n)));
+    __syncthreads();
+    fft_tile<C, N, +1, TL::L, TL::LP>(sm, tw);
+    for (int n = threadIdx.x / TL::L; n < N; n += TL::NT / TL::L) psi[q + n * S] = sm[n * TL::LP + l];
+}
+
+// P7: x-pass forward on the half spectrum, multiply by -1/kappa^2 (0 at k=0),
+// x-pass inverse.
+template <typename R, int N>
+__global__ void __launch_bounds__(Tile<R, N>::NT)
+    k_fft_x_poisson(cx<R> *__restrict__ rhok, const cx<R> *__restrict__ tw) {
+    using C = cx<R>;
+    using TL = Tile<R, N>;
+    constexpr int NH = N / 2 + 1;
+    constexpr int NHP = half_pitch<R>(N);
+    extern __shared__ __align__(16) unsigned char smraw[];
+    C *sm = reinterpret_cast<C *>(smraw);
+    const int l = threadIdx.x % TL::L;
+    const long q = long(blockIdx.x) * TL::L + l;  // column = y*NHP + kz
+    const int y = int(q / NHP), kz = int(q % NHP);
+    const bool valid = kz < NH;
+    const size_t S = size_t(N) * NHP;
+    for (int n = threadIdx.x / TL::L; n < N; n += TL::NT / TL::L)
+        sm[n * TL::LP + l] = valid ? rhok[q + n * S] : mkc(R(0), R(0));
+    __syncthreads();
+    fft_tile<C, N, -1, TL::L, TL::LP>(sm, tw);
+    const int ky = kappa(y, N), kzz = kappa(kz, N);
+    const int k2yz = ky * ky + kzz * kzz;
+    for (int n = threadIdx.x / TL::L; n < N; n += TL::NT / TL::L) {
+        const int kx = kappa(n, N);
+        const int k2 = kx * kx + k2yz;
+        const R m = k2 == 0 ? R(0) : R(-1) / R(k2);
+        sm[n * TL::LP + l] = cscale(sm[n * TL::LP + l], m);
+    }
+    __syncthreads();
+    fft_tile<C, N, +1, TL::L, TL::LP>(sm, tw);
+    if (valid)
+        for (int n = threadIdx.x / TL::L; n < N; n += TL::NT / TL::L) rhok[q + n * S] = sm[n * TL::LP + l];
+}
+
+// ------------------------------------------------------- state transfer ---
+// out = S * psi_s * exp(-i (cP phi_s + cQ |psi_s|^2)) as complex128; the
+// coefficients are read from the TState field pair selected by `which`
+// (0: none, 1: snapshot kick, 2: pending kick).
+template <typename R>
+__global__ void k_psi_out(const cx<R> *__restrict__ psi, const R *__restrict__ phi, const TState *__restrict__ ts,
+                          int which, double S, double2 *__restrict__ out, size_t n) {
+    const double cp = which == 1 ? ts->snapP : (which == 2 ? ts->pendP : 0.0);
+    const double cq = which == 1 ? ts->snapQ : (which == 2 ? ts->pendQ : 0.0);
+    for (size_t i = size_t(blockIdx.x) * blockDim.x + threadIdx.x; i < n; i += size_t(gridDim.x) * blockDim.x) {
+        const cx<R> v = psi[i];
+        double2 w = make_double2((double)v.x, (double)v.y);
+        if (which) {
+            const double p = cp * (double)phi[i] + cq * (w.x * w.x + w.y * w.y);
+            double s, c;
+            sincos(p, &s, &c);
+            w = make_double2(w.x * c + w.y * s, w.y * c - w.x * s);
+        }
+        out[i] = make_double2(w.x * S, w.y * S);
+    }
+}
+
+template <typename R>
+__global__ void k_psi_in(const double2 *__restrict__ in, cx<R> *__restrict__ psi, double invS, size_t n) {
+    for (size_t i = size_t(blockIdx.x) * blockDim.x + threadIdx.x; i < n; i += size_t(gridDim.x) * blockDim.x) {
+        const double2 v = in[i];
+        psi[i] = mkc((R)(v.x * invS), (R)(v.y * invS));
+    }
+}
+
+template <typename R>
+__global__ void k_phi_out(const R *__restrict__ phi, double Phi0, double *__restrict__ out, size_t n) {
+    for (size_t i = size_t(blockIdx.x) * blockDim.x + threadIdx.x; i < n; i += size_t(gridDim.x) * blockDim.x)
+        out[i] = (double)phi[i] * Phi0;
+}
+
+}  // namespace ifdm

@@ -1,0 +1,155 @@
+"""Python mirror of the reference's run interface over the C ABI.
+
+``Simulation`` takes the reference's 10 run-time parameters
+(``src/CosmoBEC_MPI.cpp:329-339``) and exposes its phases: IC generation
+(``Gadget_IC_Generator``), rerun (``read_rerun``), the stepping loop with its
+snapshot state machine (``Simulation``), snapshot writes (``writeall``), plus
+fixed-step stepping and state access for tests and benchmarks.
+"""
+
+from __future__ import annotations
+
+import ctypes as C
+
+import numpy as np
+
+from . import _lib
+from ._lib import IfdmError, Params, State
+
+
+def _check(lib, h, rc: int) -> int:
+    if rc < 0:
+        msg = lib.ifdm_last_error(h)
+        raise IfdmError(rc, msg.decode() if msg else "")
+    return rc
+
+
+class Simulation:
+    """One box on one GPU.
+
+    precision: "fp64" (the drop-in path) or "fp32" (FP32-mixed).
+    ic_mode:   "ref1" reproduces the reference run on one MPI rank, "exact"
+               deposits every IC particle once.
+    """
+
+    def __init__(self, mfdm: float, g: float, xmax: float, res: int, t_write: int = 1, t_stop: int = 1,
+                 ti: int = 0, opath: str = "", icpath: str = "", rerun: int = 0, precision: str = "fp64",
+                 stan: bool = False, ic_mode: str = "ref1", device: int = 0, verbose: bool = False):
+        self.lib = _lib.load_library()
+        self._strs = [opath.encode(), icpath.encode()]
+        p = Params()
+        self.lib.ifdm_params_default(C.byref(p))
+        p.mfdm, p.g, p.xmax, p.res = mfdm, g, xmax, res
+        p.t_write, p.t_stop, p.ti = t_write, t_stop, ti
+        p.opath, p.icpath, p.rerun = self._strs[0], self._strs[1], rerun
+        p.precision = {"fp64": _lib.FP64, "fp32": _lib.FP32}[precision]
+        p.stan = int(stan)
+        p.ic_mode = {"ref1": _lib.IC_REF1, "exact": _lib.IC_EXACT}[ic_mode]
+        p.device = device
+        p.verbose = int(verbose)
+        self.N = res
+        self.precision = precision
+        h = C.c_void_p()
+        rc = self.lib.ifdm_create(C.byref(p), C.byref(h))
+        self.h = h.value
+        if rc < 0:
+            msg = self.lib.ifdm_last_error(self.h)
+            self.close()
+            raise IfdmError(rc, msg.decode() if msg else "")
+
+    def close(self) -> None:
+        if getattr(self, "h", None):
+            self.lib.ifdm_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        self.close()
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *exc):
+        self.close()
+
+    def _c(self, rc: int) -> int:
+        return _check(self.lib, self.h, rc)
+
+    # ---------------------------------------------------------------- state --
+    def load_ic(self) -> None:
+        self._c(self.lib.ifdm_load_ic(self.h))
+
+    def load_snapshot(self, t: int) -> None:
+        self._c(self.lib.ifdm_load_snapshot(self.h, t))
+
+    def set_psi(self, psi, a: float, rhoc: float = 0.0) -> None:
+        """psi: complex128 array (host numpy) or CUDA tensor of N^3 elements."""
+        if hasattr(psi, "data_ptr"):
+            ptr = psi.data_ptr()
+            self._c(self.lib.ifdm_set_psi(self.h, C.c_void_p(ptr), a, rhoc))
+        else:
+            buf = np.ascontiguousarray(psi, dtype=np.complex128)
+            self._c(self.lib.ifdm_set_psi(self.h, buf.ctypes.data_as(C.c_void_p), a, rhoc))
+
+    def get_psi(self, out: np.ndarray | None = None) -> np.ndarray:
+        if out is None:
+            out = np.empty((self.N,) * 3, dtype=np.complex128)
+        self._c(self.lib.ifdm_get_psi(self.h, out.ctypes.data_as(C.c_void_p)))
+        return out
+
+    def get_phi(self) -> np.ndarray:
+        out = np.empty((self.N,) * 3, dtype=np.float64)
+        self._c(self.lib.ifdm_get_phi(self.h, out.ctypes.data_as(C.c_void_p)))
+        return out
+
+    def state(self) -> dict:
+        s = State()
+        self._c(self.lib.ifdm_get_state(self.h, C.byref(s)))
+        return {k: getattr(s, k) for k, _ in State._fields_}
+
+    # ------------------------------------------------------------- stepping --
+    def run(self) -> None:
+        self._c(self.lib.ifdm_run(self.h))
+
+    def step(self, nsteps: int, dt_scale: float = 1.0) -> None:
+        self._c(self.lib.ifdm_step(self.h, nsteps, dt_scale))
+
+    def write_snapshot(self, t: int) -> None:
+        self._c(self.lib.ifdm_write_snapshot(self.h, t))
+
+    def synchronize(self) -> None:
+        self._c(self.lib.ifdm_synchronize(self.h))
+
+    @property
+    def stream(self) -> int:
+        return self.lib.ifdm_stream(self.h) or 0
+
+    def profile_passes(self, nsteps: int, dt_scale: float = 1.0) -> dict:
+        ms = (C.c_double * 16)()
+        names = (C.c_char_p * 16)()
+        n = self._c(self.lib.ifdm_profile_passes(self.h, nsteps, dt_scale, ms, names, 16))
+        return {names[i].decode(): ms[i] for i in range(n)}
+
+    def pass_bytes(self) -> list[float]:
+        b = (C.c_double * 16)()
+        n = self._c(self.lib.ifdm_pass_bytes(self.h, b, 16))
+        return [b[i] for i in range(n)]
+
+
+def fft3d_(tensor, sign: int) -> None:
+    """In-place unnormalised 3-D FFT of a contiguous cubic CUDA complex tensor
+    (complex128 or complex64) on torch's current stream."""
+    import torch
+
+    lib = _lib.load_library()
+    if not tensor.is_cuda or not tensor.is_contiguous() or tensor.dim() != 3:
+        raise ValueError("need a contiguous 3-D CUDA tensor")
+    n = tensor.shape[0]
+    prec = {torch.complex128: _lib.FP64, torch.complex64: _lib.FP32}[tensor.dtype]
+    stream = torch.cuda.current_stream(tensor.device).cuda_stream
+    rc = lib.ifdm_fft3d(C.c_void_p(tensor.data_ptr()), n, prec, sign, C.c_void_p(stream))
+    if rc < 0:
+        raise IfdmError(rc, "ifdm_fft3d failed")
+
+
+def supported_res(res: int, precision: str = "fp64") -> bool:
+    return bool(_lib.load_library().ifdm_supported_res(res, {"fp64": 0, "fp32": 1}[precision]))

@@ -141,3 +141,47 @@ def read_gadget_chunk(path: str):
     off += 8 + 12 * n
     vel = np.frombuffer(raw, dtype="<f4", count=3 * n, offset=off + 4).reshape(n, 3)
     return hdr, pos, vel
+
+
+def zeldovich_psi(N: int, xmax: float = 5.0, seed: int = 0, a: float = 1.0 / 51.0, rms_delta: float = 0.02,
+                  mfdm: float = 2.5e-24, slope: float = -2.5, workers: int = -1) -> np.ndarray:
+    """psi at the IC in the reference's units, built on the grid directly.
+
+    Field-level form of the particle recipe above, for grids where writing
+    N^3 particles is impractical (the benchmark's 512^3): the CIC density of
+    the Zel'dovich lattice is rho = rho_c (1 + delta) to first order, and the
+    reference's phase solve (src/gadget_IC.h:157-247) turns the linear
+    velocity v = vfac s into theta = a^{3/2} uc vfac/(1000 h) grad^-2 delta
+    (kpc/h gradients).  psi = 1.225 sqrt(rho / m_solar) exp(i m/(c^2 hbar) theta)
+    as in src/gadget_IC.h:666, rho in Msun/Mpc^3.
+    """
+    import scipy.fft as sfft
+
+    box = 2.0 * xmax * 1e3
+    Lg = box / N
+    rng = np.random.default_rng(seed)
+    wk = sfft.rfftn(rng.standard_normal((N, N, N), dtype=np.float64), workers=workers)
+    kf = (2.0 * np.pi * np.fft.fftfreq(N, d=Lg)).astype(np.float64)
+    kr = (2.0 * np.pi * np.fft.rfftfreq(N, d=Lg)).astype(np.float64)
+    k2 = kf[:, None, None] ** 2 + kf[None, :, None] ** 2 + kr[None, None, :] ** 2
+    k2[0, 0, 0] = 1.0
+    wk *= k2 ** (slope / 4.0)
+    wk[0, 0, 0] = 0.0
+    delta = sfft.irfftn(wk, s=(N, N, N), workers=workers)
+    scale = rms_delta / delta.std()
+    delta *= scale
+    wk *= -scale / k2
+    pot = sfft.irfftn(wk, s=(N, N, N), workers=workers)  # grad^-2 delta, (kpc/h)^2
+    del wk, k2
+    E = np.sqrt(OMEGA_M0 / a**3 + 1.0 - OMEGA_M0)
+    f = (OMEGA_M0 / a**3 / E**2) ** 0.55
+    vfac = np.sqrt(a) * 100.0 * E * f / 1000.0
+    m2Mpc, s2Myr = 3.086e22, 60.0 * 60.0 * 24.0 * 365.0 * 1e6
+    uc = 1e3 / m2Mpc * s2Myr
+    hbar = 6.58211928e-16 / s2Myr
+    c = 2.99792458e8 / m2Mpc * s2Myr
+    mfdm_solar = mfdm * 1.783e-36 / 1.989e30
+    theta = a**1.5 * uc * vfac / (1000.0 * H_LITTLE) * pot
+    phase = (mfdm / c**2 / hbar) * theta
+    amp = 1.225 * np.sqrt(np.maximum(RHOC * (1.0 + delta), 0.0) / mfdm_solar)
+    return (amp * np.exp(1j * phase)).astype(np.complex128)

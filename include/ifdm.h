@@ -1,0 +1,142 @@
+/*
+ * include/ifdm.h -- C ABI of libifdm_b200.so, the B200 (sm_100a) build of
+ * IFDM_Code's leap-frog pseudo-spectral Schroedinger-Poisson step.
+ *
+ * The reference has no library interface: its drop-in surface is the
+ * executable (`BECMPI.o mfdm g xmax res t_write t_stop ti opath icpath rerun`,
+ * src/CosmoBEC_MPI.cpp:313-379), the Gadget IC chunk files
+ * (src/gadget_IC.h:259-353), the snapshot files (src/write3D.h:7-97) and
+ * stdout.  Each entry point below names the reference function it replaces.
+ * Paths cited are relative to the reference project.
+ *
+ * Conventions
+ *  - Every function returns IFDM_OK (0) or a negative IFDM_ERR_* code and
+ *    never exits the process; ifdm_last_error() gives the message.
+ *  - Host arrays are caller-owned.  psi is N^3 complex128 as interleaved
+ *    (re, im) doubles, x slowest and z fastest (the reference's
+ *    opr.wfc[k + N*(j + N*i)], src/CosmoBEC_MPI.cpp:133).
+ *  - A context owns its device buffers and CUDA stream; one host thread at a
+ *    time may use a context.
+ */
+#ifndef IFDM_H
+#define IFDM_H
+
+#include <stddef.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define IFDM_OK 0
+#define IFDM_ERR_ARGS (-1)        /* bad argument count / value */
+#define IFDM_ERR_CUDA (-2)        /* CUDA runtime error */
+#define IFDM_ERR_IO (-3)          /* missing or truncated file */
+#define IFDM_ERR_BOXSIZE (-4)     /* IC box differs from 2*xmax (src/gadget_IC.h:309-314) */
+#define IFDM_ERR_UNSUPPORTED (-5) /* grid size without a compiled plan */
+#define IFDM_ERR_STATE (-6)       /* call out of order (e.g. step before a psi exists) */
+#define IFDM_ERR_DEVICE (-7)      /* a device-side check failed (bounded wait, quadrature limit) */
+
+enum ifdm_precision { IFDM_FP64 = 0, IFDM_FP32 = 1 };
+/* IC deposit: REF1 reproduces the reference run on one MPI rank (particles in
+ * the last half cell deposited twice, one zero particle per chunk at the
+ * origin: src/gadget_IC.h:431-448,496-510); EXACT deposits each particle once
+ * (what the reference does on many ranks, apart from its rank-boundary
+ * off-by-one at src/gadget_IC.h:434-435). */
+enum ifdm_ic_mode { IFDM_IC_REF1 = 0, IFDM_IC_EXACT = 1 };
+
+/* The reference's 10 run-time parameters (src/CosmoBEC_MPI.cpp:329-339,
+ * README.md:8-21) plus B200 options. */
+typedef struct ifdm_params {
+    double mfdm;       /* particle mass [eV]                      argv[1] */
+    double g;          /* self-interaction [eV cm^3]              argv[2] */
+    double xmax;       /* half box [Mpc/h]                        argv[3] */
+    int res;           /* grid points per axis                    argv[4] */
+    int t_write;       /* snapshot period [steps]                 argv[5] */
+    int t_stop;        /* last step (exclusive)                   argv[6] */
+    int ti;            /* first step / rerun snapshot number      argv[7] */
+    const char *opath; /* output prefix (trailing '/')            argv[8] */
+    const char *icpath;/* IC prefix, or snapshot dir when rerun   argv[9] */
+    int rerun;         /* 1: start from <icpath>output<ti>.dat    argv[10] */
+    int precision;     /* IFDM_FP64 (drop-in) or IFDM_FP32 (mixed) */
+    int stan;          /* 1: snapshot state machine of src/CosmoBEC_MPI_stan.cpp */
+    int ic_mode;       /* enum ifdm_ic_mode */
+    int device;        /* CUDA device ordinal */
+    int verbose;       /* 1: print the reference's per-step stdout lines */
+} ifdm_params;
+
+/* Scalars of the time integration after the latest step. */
+typedef struct ifdm_state {
+    double a;          /* scale factor (par.ai) */
+    double dt_KE, dt_PE, dt_QI; /* integrated step weights (src/CosmoBEC_MPI.cpp:66-68) */
+    double max_phi;    /* max |phi| over the reference's scan window */
+    double max_rho;    /* max |psi|^2 */
+    double rhoc;       /* mean density subtracted in the Poisson source */
+    long long steps;   /* leap-frog steps taken by this context */
+    int criterion;     /* 3: kinetic, 2: potential, 4: self-interaction limited */
+    int device_error;  /* nonzero when a device-side check failed */
+} ifdm_state;
+
+typedef struct ifdm_ctx ifdm_ctx;
+
+/* Fill defaults: FP64, stan 0, IFDM_IC_REF1, device 0, verbose 0. */
+void ifdm_params_default(ifdm_params *p);
+
+/* Parse argv exactly as main() does (src/CosmoBEC_MPI.cpp:324-340): argc must
+ * be 11; numbers via atof/atoi.  The strings point into argv. */
+int ifdm_params_from_argv(int argc, char **argv, ifdm_params *p);
+
+/* Allocate a context on p->device (Params/Operators, src/struct3D.h:17-125). */
+int ifdm_create(const ifdm_params *p, ifdm_ctx **out);
+void ifdm_destroy(ifdm_ctx *ctx);
+const char *ifdm_last_error(const ifdm_ctx *ctx);
+/* 1 if `res` has a compiled FFT plan for `precision`. */
+int ifdm_supported_res(int res, int precision);
+
+/* Gadget_IC_Generator (src/gadget_IC.h:686-707): read <icpath>.0..3, CIC
+ * deposit, velocity-divergence phase, psi = 1.225 sqrt(rho h^2 1e9/m) e^{i..};
+ * also writes <opath>voutput.dat (src/write3D.h:24-53). */
+int ifdm_load_ic(ifdm_ctx *ctx);
+/* read_rerun (src/gadget_IC.h:709-750): psi and a from <icpath>output<t>.dat. */
+int ifdm_load_snapshot(ifdm_ctx *ctx, int t);
+/* Start from a host psi (complex128, N^3) at scale factor a; rhoc <= 0 means
+ * the constant 3.51059e10 that read_rerun uses. */
+int ifdm_set_psi(ifdm_ctx *ctx, const double *psi, double a, double rhoc);
+/* psi after the latest full step (the pending second half-kick applied). */
+int ifdm_get_psi(ifdm_ctx *ctx, double *psi);
+/* phi (N^3 doubles) of the current density. */
+int ifdm_get_phi(ifdm_ctx *ctx, double *phi);
+int ifdm_get_state(ifdm_ctx *ctx, ifdm_state *out);
+
+/* Simulation (src/CosmoBEC_MPI.cpp:183-310): steps ti..t_stop-1 with the
+ * adaptive timestep, the snapshot state machine and its early stops. */
+int ifdm_run(ifdm_ctx *ctx);
+/* Fixed-step mode: nsteps leap-frog steps, no snapshots or stops, the
+ * selected timestep multiplied by dt_scale (1.0 = the reference's rule).
+ * Asynchronous on the context's stream. */
+int ifdm_step(ifdm_ctx *ctx, int nsteps, double dt_scale);
+/* writeall (src/write3D.h:86-97): <opath>output<t>.dat of the current state. */
+int ifdm_write_snapshot(ifdm_ctx *ctx, int t);
+int ifdm_synchronize(ifdm_ctx *ctx);
+/* The context's cudaStream_t (as void*). */
+void *ifdm_stream(ifdm_ctx *ctx);
+
+/* Average device time per leap-frog step of each fused pass over `nsteps`
+ * fixed-mode steps (CUDA events on the context's stream).  ms_out receives
+ * up to `cap` entries; names_out (optional) gets static pass names.
+ * Returns the number of passes. */
+int ifdm_profile_passes(ifdm_ctx *ctx, int nsteps, double dt_scale, double *ms_out, const char **names_out,
+                        int cap);
+/* Algorithmic HBM bytes one step moves, per pass (same order as above). */
+int ifdm_pass_bytes(ifdm_ctx *ctx, double *bytes_out, int cap);
+
+/* Device-pointer transforms on the caller's stream (cudaStream_t as void*).
+ * In-place unnormalised 3-D complex FFT of data[n][n][n] (complex128 when
+ * precision == IFDM_FP64, complex64 otherwise); sign -1 forward, +1 backward
+ * -- the contract of the reference's fftw_mpi_plan_dft_3d plans
+ * (src/CosmoBEC_MPI.cpp:176-177). */
+int ifdm_fft3d(void *data, int n, int precision, int sign, void *stream);
+
+#ifdef __cplusplus
+}
+#endif
+#endif

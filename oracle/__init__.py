@@ -11,4 +11,4 @@ package ``ifdm_code_b200`` never imports it.
   reference tree when it is present.
 """
 
-from .pyoracle import Oracle, OracleArgs, build, ref_binary, oracle_constants  # noqa: F401
+from .pyoracle import IC_EXACT, IC_REF1, Oracle, OracleArgs, build, oracle_constants, ref_binary  # noqa: F401

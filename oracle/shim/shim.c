@@ -10,6 +10,7 @@
 #include <stdlib.h>
 #include <string.h>
 #include <sys/stat.h>
+#include <time.h>
 #include <unistd.h>
 
 #include "../fft64.h"
@@ -39,8 +40,28 @@ int MPI_Comm_rank(MPI_Comm c, int *r) { (void)c; *r = 0; return 0; }
 int MPI_Comm_size(MPI_Comm c, int *s) { (void)c; *s = 1; return 0; }
 int MPI_Barrier(MPI_Comm c) { (void)c; return 0; }
 
+/* Timestep_criteria makes exactly two Allreduce calls per step
+ * (src/CosmoBEC_MPI.cpp:29-30); with IFDM_SHIM_TIMING=<file> each call appends
+ * a CLOCK_MONOTONIC timestamp, which times the reference's own step loop. */
+static void shim_timestamp(void) {
+    static FILE *tf = NULL;
+    static int checked = 0;
+    if (!checked) {
+        checked = 1;
+        const char *path = getenv("IFDM_SHIM_TIMING");
+        if (path && *path) tf = fopen(path, "w");
+    }
+    if (tf) {
+        struct timespec ts;
+        clock_gettime(CLOCK_MONOTONIC, &ts);
+        fprintf(tf, "%lld.%09ld\n", (long long)ts.tv_sec, ts.tv_nsec);
+        fflush(tf);
+    }
+}
+
 int MPI_Allreduce(const void *sendbuf, void *recvbuf, int count, MPI_Datatype dt, MPI_Op op, MPI_Comm c) {
     (void)op; (void)c;
+    shim_timestamp();
     if (sendbuf != recvbuf) memmove(recvbuf, sendbuf, (size_t)count * dt_size(dt));
     return 0;
 }

@@ -149,6 +149,24 @@ def time_steps(sim, steps: int, warmup: int, dt_scale: float, torch):
     return e0.elapsed_time(e1)
 
 
+def power_spectrum(rho, nbins: int = 24):
+    """Spherically averaged P(k) of the density contrast, log-spaced |k| bins."""
+    import numpy as np
+    import scipy.fft as sfft
+
+    N = rho.shape[0]
+    d = rho / rho.mean() - 1.0
+    pk = np.abs(sfft.rfftn(d, workers=-1)) ** 2
+    k = np.fft.fftfreq(N) * N
+    kr = np.fft.rfftfreq(N) * N
+    kk = np.sqrt(k[:, None, None] ** 2 + k[None, :, None] ** 2 + kr[None, None, :] ** 2)
+    edges = np.logspace(0, np.log10(N / 2), nbins + 1)
+    idx = np.digitize(kk.ravel(), edges)
+    sums = np.bincount(idx, weights=pk.ravel(), minlength=nbins + 2)[1:nbins + 1]
+    cnt = np.bincount(idx, minlength=nbins + 2)[1:nbins + 1]
+    return sums[cnt > 0] / cnt[cnt > 0]
+
+
 def cpu_baseline_port(N: int, psi0, dt_scale: float):
     """The oracle (C restatement, OpenMP on every host core) for one step at N^3."""
     from oracle import Oracle, OracleArgs
@@ -202,32 +220,55 @@ def run_ours(args):
         return float(t.item())
 
     res = {}
-    for prec in ("fp32", "fp64"):
+    for prec in ("fp64", "mixed", "fp32"):
         sim = ifdm.Simulation(MFDM, 0.0, XMAX, N, precision=prec, device=local)
         sim.set_psi(psi0, A0)
         sim.step(W, C)
         sim.synchronize()
         barrier()
-        clk = ClockSampler(local) if prec == "fp32" else None
-        if clk:
-            clk.__enter__()
-        ms = time_steps(sim, K, 0, C, torch)
-        if clk:
-            clk.__exit__()
+        clk = ClockSampler(local)
+        with clk:
+            ms = time_steps(sim, K, 0, C, torch)
         barrier()
         ms = max_over_ranks(ms)
         prof = sim.profile_passes(max(3, min(10, K)), C)
         pb = sim.pass_bytes()
         st = sim.state()
-        res[prec] = dict(ms=ms, prof=prof, bytes=pb, state=st, clocks=clk.summary() if clk else None)
+        res[prec] = dict(ms=ms, prof=prof, bytes=pb, state=st, clocks=clk.summary())
+        if args.precision_steps > 0:
+            # the precision gate: density after `precision_steps` steps from the IC
+            sim.set_psi(psi0, A0)
+            sim.step(args.precision_steps, C)
+            res[prec]["rho"] = np.abs(sim.get_psi()) ** 2
+            res[prec]["a_end"] = sim.state()["a"]
         sim.close()
         del sim
         torch.cuda.synchronize()
+    prec_report = {}
+    if args.precision_steps > 0:
+        ref = res["fp64"]["rho"]
+        pk_ref = power_spectrum(ref)
+        for prec in ("mixed", "fp32"):
+            rho = res[prec]["rho"]
+            pk = power_spectrum(rho)
+            prec_report[prec] = {
+                "steps": args.precision_steps,
+                "density_relL2": float(np.linalg.norm(rho - ref) / np.linalg.norm(ref)),
+                "norm_drift": float(rho.sum() / ref.sum() - 1.0),
+                "pk_ratio_max_dev": float(np.max(np.abs(pk / pk_ref - 1.0))),
+                "a_end": res[prec]["a_end"],
+            }
+            del res[prec]["rho"]
+        del res["fp64"]["rho"]
+    gate = 1e-5
+    head = "mixed"
+    if prec_report and prec_report["mixed"]["density_relL2"] > gate:
+        head = "fp32" if prec_report["fp32"]["density_relL2"] <= gate else "fp64"
 
     # end to end through the C ABI with host buffers (pinned)
     pin_in = torch.from_numpy(psi0.view(np.float64)).pin_memory()
     pin_out = torch.empty_like(pin_in).pin_memory()
-    sim = ifdm.Simulation(MFDM, 0.0, XMAX, N, precision="fp32", device=local)
+    sim = ifdm.Simulation(MFDM, 0.0, XMAX, N, precision=head, device=local)
     sim.set_psi(pin_in.numpy().view(np.complex128), A0)
     sim.step(W, C)
     sim.synchronize()
@@ -241,8 +282,9 @@ def run_ours(args):
     e2e_s = max_over_ranks(e2e_s)
 
     cells = float(N) ** 3
-    value = world * cells * K / (res["fp32"]["ms"] / 1e3)
-    fp64_value = world * cells * K / (res["fp64"]["ms"] / 1e3)
+    value = world * cells * K / (res[head]["ms"] / 1e3)
+    vals = {p: world * cells * K / (res[p]["ms"] / 1e3) for p in res}
+    fp64_value = vals["fp64"]
     e2e_value = world * cells * K / e2e_s
 
     def roofline(r):
@@ -266,24 +308,26 @@ def run_ours(args):
         "n_gpus": world,
         "steps": K,
         "warmup": W,
-        "ms_per_step": res["fp32"]["ms"] / K,
+        "ms_per_step": res[head]["ms"] / K,
         "higher_is_better": True,
         "scaling": "weak",
         "vs_baseline": None,
-        "dtype": "f32",
+        "dtype": {"mixed": "f32 storage / f64 arithmetic", "fp32": "f32", "fp64": "f64"}[head],
+        "path": head,
         "data": "synthetic",
         "config": {"workload": f"{N}^3 leap-frog step, xmax=5 Mpc/h, mfdm=2.5e-24 eV, g=0, z=50 Zel'dovich IC, "
                                f"fixed-step dt_scale={C:.4f} (1000 steps to a=0.5)",
                    "res": N, "parallelism": f"replicas x{world}" if world > 1 else "1 box",
                    "l2": "inputs larger than L2 (psi fp32 = %.1f GB)" % (8 * cells / 1e9)},
-        "fp64": {"value": fp64_value, "unit": "cell-steps/s", "ms_per_step": res["fp64"]["ms"] / K,
-                 "fp32_over_fp64": value / fp64_value, "roofline": roofline(res["fp64"])},
-        "roofline": roofline(res["fp32"]),
+        "paths": {p: {"value": vals[p], "ms_per_step": res[p]["ms"] / K, "over_fp64": vals[p] / fp64_value,
+                      "roofline": roofline(res[p]), "clocks": res[p]["clocks"]} for p in res},
+        "precision": prec_report,
+        "roofline": roofline(res[head]),
         "e2e": {"value": e2e_value, "unit": "cell-steps/s", "h2d_bytes_per_step": 16 * cells / K,
                 "d2h_bytes_per_step": 16 * cells / K,
                 "note": f"set_psi from pinned host complex128, {K} steps, get_psi to pinned host, per step = /K"},
         "gpu_launches": 10 * K,
-        "clocks": res["fp32"]["clocks"],
+        "clocks": res[head]["clocks"],
     }
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         out["cpu_baseline"] = cpu_baseline_port(N, psi0, C)
@@ -344,20 +388,42 @@ def run_reference(args):
     }))
 
 
+def run_profile(args):
+    """Short fixed run of one precision for ncu captures: W + K steps, no timing."""
+    import ifdm_code_b200 as ifdm
+    from ifdm_code_b200.synthetic_ic import zeldovich_psi
+
+    N = args.res
+    C = dt_scale_for(N)
+    psi0 = zeldovich_psi(N, xmax=XMAX, seed=0, a=A0, mfdm=MFDM)
+    with ifdm.Simulation(MFDM, 0.0, XMAX, N, precision=args.precision) as sim:
+        sim.set_psi(psi0, A0)
+        sim.step(args.warmup + args.steps, C)
+        sim.synchronize()
+        print(json.dumps({"profile": True, "res": N, "precision": args.precision, "steps": args.warmup + args.steps,
+                          "a": sim.state()["a"]}))
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
-    ap.add_argument("--steps", type=int, default=50)
+    ap.add_argument("--steps", type=int, default=200)
     ap.add_argument("--warmup", type=int, default=5)
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
     ap.add_argument("--res", type=int, default=N_DEFAULT)
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--profile", action="store_true", help="plain W+K steps of --precision (for ncu)")
+    ap.add_argument("--precision", choices=["fp32", "fp64", "mixed"], default="mixed")
+    ap.add_argument("--precision-steps", type=int, default=1000,
+                    help="steps of the precision gate (density error vs FP64); 0 skips it")
     ap.add_argument("--ref-max-steps", type=int, default=3,
                     help="bound on timed reference steps (each is ~tens of seconds at 512^3)")
     args = ap.parse_args()
     if args.warmup < 3 and args.impl == "ours":
         args.warmup = 3
-    if args.impl == "reference":
+    if args.profile:
+        run_profile(args)
+    elif args.impl == "reference":
         run_reference(args)
     else:
         run_ours(args)

@@ -19,7 +19,7 @@ ERRORS = {
     -1: "IFDM_ERR_ARGS", -2: "IFDM_ERR_CUDA", -3: "IFDM_ERR_IO", -4: "IFDM_ERR_BOXSIZE",
     -5: "IFDM_ERR_UNSUPPORTED", -6: "IFDM_ERR_STATE", -7: "IFDM_ERR_DEVICE",
 }
-FP64, FP32 = 0, 1
+FP64, FP32, MIXED = 0, 1, 2
 IC_REF1, IC_EXACT = 0, 1
 
 # every entry point include/ifdm.h declares

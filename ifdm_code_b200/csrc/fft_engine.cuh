@@ -165,28 +165,39 @@ __device__ __forceinline__ void stockham_stage(C *sm, const C *__restrict__ tw, 
     __syncthreads();
 }
 
-template <typename C, int N, int DIR, int L, int LP, int S, int NS>
+template <typename C, int N, int E, int DIR, int L, int LP, int S, int NS>
 struct StageLoop {
     __device__ __forceinline__ static void run(C *sm, const C *__restrict__ tw, int l, int t, bool active) {
         if constexpr (S < Plan<N>::NST) {
             constexpr int RAD = Plan<N>::R[S];
-            stockham_stage<C, N, Plan<N>::E, DIR, L, LP, RAD, NS>(sm, tw, l, t, active);
-            StageLoop<C, N, DIR, L, LP, S + 1, NS * RAD>::run(sm, tw, l, t, active);
+            static_assert(E % RAD == 0, "elements per thread must be a multiple of every radix");
+            stockham_stage<C, N, E, DIR, L, LP, RAD, NS>(sm, tw, l, t, active);
+            StageLoop<C, N, E, DIR, L, LP, S + 1, NS * RAD>::run(sm, tw, l, t, active);
         }
     }
 };
 
-// Transform all L lines of the tile in place.  `nthreads` = blockDim.x; lines
-// are processed by threads tid < L * (N / E); the rest only join the barriers.
-// Caller must __syncthreads() before (tile written) -- this routine leaves the
-// tile synced.
-template <typename C, int N, int DIR, int L, int LP>
+// Elements per thread for a length-N line when T threads serve each line:
+// N / T when every radix divides it, else the plan's minimum.
+template <int N> __host__ __device__ constexpr bool divides_all(int e) {
+    for (int s = 0; s < Plan<N>::NST; ++s)
+        if (e % Plan<N>::R[s]) return false;
+    return true;
+}
+template <int N, int T> __host__ __device__ constexpr int elems_for(int) {
+    return (N % T == 0 && N / T >= Plan<N>::E && divides_all<N>(N / T)) ? N / T : Plan<N>::E;
+}
+
+// Transform all L lines of the tile in place, E elements per thread (threads
+// tid < L * (N / E) work; the rest only join the barriers).  Caller must
+// __syncthreads() before (tile written); the tile is synced on return.
+template <typename C, int N, int E, int DIR, int L, int LP>
 __device__ __forceinline__ void fft_tile(C *sm, const C *__restrict__ tw) {
-    constexpr int T = N / Plan<N>::E;
+    constexpr int T = N / E;
     const int tid = threadIdx.x;
     const int l = tid % L;
     const int t = tid / L;
-    StageLoop<C, N, DIR, L, LP, 0, 1>::run(sm, tw, l, t, t < T);
+    StageLoop<C, N, E, DIR, L, LP, 0, 1>::run(sm, tw, l, t, t < T);
 }
 
 }  // namespace ifdm

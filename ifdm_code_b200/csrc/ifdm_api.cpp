@@ -96,9 +96,9 @@ int ifdm_create(const ifdm_params *p, ifdm_ctx **out) {
         *out = c.release();
         return fail(*out, IFDM_ERR_UNSUPPORTED, "res " + std::to_string(p->res) + " has no compiled FFT plan");
     }
-    if (p->precision != IFDM_FP64 && p->precision != IFDM_FP32) {
+    if (p->precision != IFDM_FP64 && p->precision != IFDM_FP32 && p->precision != IFDM_MIXED) {
         *out = c.release();
-        return fail(*out, IFDM_ERR_ARGS, "precision must be IFDM_FP64 or IFDM_FP32");
+        return fail(*out, IFDM_ERR_ARGS, "precision must be IFDM_FP64, IFDM_FP32 or IFDM_MIXED");
     }
     using namespace phys;
     c->N = p->res;
@@ -410,7 +410,7 @@ int ifdm_pass_bytes(ifdm_ctx *c, double *bytes_out, int cap) {
 }
 
 int ifdm_fft3d(void *data, int n, int precision, int sign, void *stream) {
-    if (!data || (sign != 1 && sign != -1)) return IFDM_ERR_ARGS;
+    if (!data || (sign != 1 && sign != -1) || precision < 0 || precision > 2) return IFDM_ERR_ARGS;
     if (!supported_n(n)) return IFDM_ERR_UNSUPPORTED;
     std::string e = fft3d(data, n, precision, sign, (cudaStream_t)stream);
     return e.empty() ? IFDM_OK : IFDM_ERR_CUDA;

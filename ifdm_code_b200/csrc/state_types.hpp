@@ -12,6 +12,9 @@ struct TState {
     double snapP, snapQ;        // half kick owed by the state at this step's start (snapshots)
     double pendP, pendQ;        // half kick owed after this step's P9
     double drift_s;             // drift phase per unit kappa^2
+    double cre, cim;            // offset c removed before the forward FFT, added after the inverse
+    double cnext_re, cnext_im;  // mean of the kicked field, from the k = 0 coefficient (next step's c)
+    double mu;                  // mean |psi_s|^2 (conserved), subtracted from the Poisson source
     double maxphi, maxrho;      // natural units, inputs of the latest timestep
     unsigned long long maxphi_bits, maxrho_bits; // atomicMax targets (scaled, non-negative doubles)
     long long steps;

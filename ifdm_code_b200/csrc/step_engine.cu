@@ -3,10 +3,15 @@
 #include "physics.hpp"
 #include "step_engine.hpp"
 #include "timestep.cuh"
+#include "tma_passes.cuh"
+
+#include <cudaTypedefs.h>
 
 #include <cmath>
 #include <cstdio>
+#include <cstdlib>
 #include <cstring>
+#include <type_traits>
 
 namespace ifdm {
 
@@ -28,13 +33,16 @@ bool supported_n(int n) {
 }
 
 // ---------------------------------------------------------------- per-N ops --
-template <typename R, int N> struct Box {
-    using C = cx<R>;
-    using TL = Tile<R, N>;
+template <typename R_, typename K_, int N> struct Box {
+    using R = R_;
+    using K = K_;
+    using TL = Tile<R, K, N>;
+    using C = cx<K>;
+    using G = cx<R>;
     static constexpr int NH = N / 2 + 1;
     static constexpr int NHP = half_pitch<R>(N);
     static constexpr size_t SM = TL::SMEM;
-    static constexpr size_t SM9 = size_t(N + 1) * TL::LP * sizeof(C);
+    static constexpr size_t SM9 = TL::SMEM9;
     // every launch covers its array exactly: no partial tiles
     static_assert((N * N) % TL::L == 0, "z/y/x tiles must divide N^2 lines");
     static_assert((N * NHP) % TL::L == 0, "half-spectrum tiles must divide N*NHP lines");
@@ -42,86 +50,153 @@ template <typename R, int N> struct Box {
     static_assert(TL::NT <= 1024, "block size");
     static_assert(SM9 <= 227 * 1024, "shared memory per block");
 
-    template <typename K> static cudaError_t prep(K kern, size_t smem) {
+    template <typename Kern> static cudaError_t prep(Kern kern, size_t smem) {
         return cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
     }
 
     static std::string configure() {
         static bool done = false;
         if (done) return "";
-        CUDA_TRY(prep(k_kick_fft_z<R, N>, SM));
-        CUDA_TRY(prep(k_fft_yx<R, N, -1, 1>, SM));
-        CUDA_TRY(prep(k_fft_yx<R, N, +1, 1>, SM));
-        CUDA_TRY(prep(k_fft_yx<R, N, -1, 2>, SM));
-        CUDA_TRY(prep(k_fft_yx<R, N, +1, 2>, SM));
-        CUDA_TRY(prep(k_fft_x_drift<R, N>, SM));
-        CUDA_TRY(prep(k_density_r2c_z<R, N, true>, SM));
-        CUDA_TRY(prep(k_density_r2c_z<R, N, false>, SM));
-        CUDA_TRY(prep(k_fft_x_poisson<R, N>, SM));
-        CUDA_TRY(prep(k_c2r_z_phi<R, N>, SM9));
-        CUDA_TRY(prep(k_fft_z<R, N, -1>, SM));
-        CUDA_TRY(prep(k_fft_z<R, N, +1>, SM));
+        CUDA_TRY(prep(k_kick_fft_z<R, K, N>, SM));
+        CUDA_TRY(prep(k_fft_yx<R, K, N, -1, 1>, SM));
+        CUDA_TRY(prep(k_fft_yx<R, K, N, +1, 1>, SM));
+        CUDA_TRY(prep(k_fft_yx<R, K, N, -1, 2>, SM));
+        CUDA_TRY(prep(k_fft_yx<R, K, N, +1, 2>, SM));
+        CUDA_TRY(prep(k_fft_x_drift<R, K, N>, SM));
+        CUDA_TRY(prep(k_density_r2c_z<R, K, N, true>, SM));
+        CUDA_TRY(prep(k_density_r2c_z<R, K, N, false>, SM));
+        CUDA_TRY(prep(k_fft_x_poisson<R, K, N>, SM));
+        CUDA_TRY(prep(k_c2r_z_phi<R, K, N>, SM9));
+        CUDA_TRY(prep(k_fft_z<R, K, N, -1>, SM));
+        CUDA_TRY(prep(k_fft_z<R, K, N, +1>, SM));
+        if constexpr (kTma) {
+            CUDA_TRY(prep(k_yx_tma<R, N, 1, 0, -1>, TT::SMEM));
+            CUDA_TRY(prep(k_yx_tma<R, N, 1, 0, +1>, TT::SMEM));
+            CUDA_TRY(prep(k_yx_tma<R, N, 2, 1, 0>, TT::SMEM));
+            CUDA_TRY(prep(k_yx_tma<R, N, 2, 2, 0>, TT::SMEM));
+        }
         done = true;
         return "";
     }
 
+    // TMA-pipelined y/x passes: FP32 and FP64 modes (R == K), N >= 128
+    static constexpr bool kTma = std::is_same<R, K>::value && N >= 128;
+    using TT = TmaTile<R, N>;
+
     static unsigned zblocks() { return unsigned(size_t(N) * N / TL::L); }
     static unsigned hblocks() { return unsigned(size_t(N) * NHP / TL::L); }
 
-    // one pass by index 1..9
-    static void pass(int p, cudaStream_t s, C *psi, R *phi, C *rhok, TState *ts, const C *drift, const C *tw,
-                     const C *twh, double mu, long wr, int wt) {
+    // one pass by index 1..9; tm: TMA maps (psi y, psi x, rho y, rho x) or null
+    static void pass(int p, cudaStream_t s, G *psi, R *phi, G *rhok, TState *ts, const C *drift, const C *tw,
+                     const C *twh, long wr, int wt, const CUtensorMap *tm = nullptr, int grid = 0) {
         const unsigned nt = TL::NT;
+        if constexpr (kTma) {
+            if (tm && (p == 2 || p == 3 || p == 4 || p == 6 || p == 7 || p == 8)) {
+                const int tc = int(size_t(N) * N / TT::L), th = int(size_t(N) * NHP / TT::L);
+                const unsigned g2 = unsigned(grid), tn = TT::NT;
+                const size_t sm = TT::SMEM;
+                const G *dG = reinterpret_cast<const G *>(drift);
+                switch (p) {
+                    case 2: k_yx_tma<R, N, 1, 0, -1><<<g2, tn, sm, s>>>(tm[0], psi, N, N, tc, ts, 2, dG, tw); break;
+                    case 3: k_yx_tma<R, N, 2, 1, 0><<<g2, tn, sm, s>>>(tm[1], psi, N, N, tc, ts, 3, dG, tw); break;
+                    case 4: k_yx_tma<R, N, 1, 0, +1><<<g2, tn, sm, s>>>(tm[0], psi, N, N, tc, ts, 4, dG, tw); break;
+                    case 6: k_yx_tma<R, N, 1, 0, -1><<<g2, tn, sm, s>>>(tm[2], rhok, NHP, NH, th, ts, 6, dG, tw); break;
+                    case 7: k_yx_tma<R, N, 2, 2, 0><<<g2, tn, sm, s>>>(tm[3], rhok, NHP, NH, th, ts, 7, dG, tw); break;
+                    case 8: k_yx_tma<R, N, 1, 0, +1><<<g2, tn, sm, s>>>(tm[2], rhok, NHP, NH, th, ts, 8, dG, tw); break;
+                }
+                return;
+            }
+        }
         switch (p) {
-            case 1: k_kick_fft_z<R, N><<<zblocks(), nt, SM, s>>>(psi, phi, ts, tw); break;
-            case 2: k_fft_yx<R, N, -1, 1><<<zblocks(), nt, SM, s>>>(psi, N, N, tw); break;
-            case 3: k_fft_x_drift<R, N><<<zblocks(), nt, SM, s>>>(psi, drift, tw); break;
-            case 4: k_fft_yx<R, N, +1, 1><<<zblocks(), nt, SM, s>>>(psi, N, N, tw); break;
-            case 5: k_density_r2c_z<R, N, true><<<zblocks(), nt, SM, s>>>(psi, rhok, ts, mu, tw, twh); break;
-            case 6: k_fft_yx<R, N, -1, 1><<<hblocks(), nt, SM, s>>>(rhok, NHP, NH, tw); break;
-            case 7: k_fft_x_poisson<R, N><<<hblocks(), nt, SM, s>>>(rhok, tw); break;
-            case 8: k_fft_yx<R, N, +1, 1><<<hblocks(), nt, SM, s>>>(rhok, NHP, NH, tw); break;
-            case 9: k_c2r_z_phi<R, N><<<zblocks(), nt, SM9, s>>>(rhok, phi, ts, wr, wt, tw, twh); break;
+            case 1: k_kick_fft_z<R, K, N><<<zblocks(), nt, SM, s>>>(psi, phi, ts, tw); break;
+            case 2: k_fft_yx<R, K, N, -1, 1><<<zblocks(), nt, SM, s>>>(psi, N, N, ts, 2, tw); break;
+            case 3: k_fft_x_drift<R, K, N><<<zblocks(), nt, SM, s>>>(psi, drift, ts, tw); break;
+            case 4: k_fft_yx<R, K, N, +1, 1><<<zblocks(), nt, SM, s>>>(psi, N, N, ts, 4, tw); break;
+            case 5: k_density_r2c_z<R, K, N, true><<<zblocks(), nt, SM, s>>>(psi, rhok, ts, nullptr, tw, twh); break;
+            case 6: k_fft_yx<R, K, N, -1, 1><<<hblocks(), nt, SM, s>>>(rhok, NHP, NH, ts, 6, tw); break;
+            case 7: k_fft_x_poisson<R, K, N><<<hblocks(), nt, SM, s>>>(rhok, ts, tw); break;
+            case 8: k_fft_yx<R, K, N, +1, 1><<<hblocks(), nt, SM, s>>>(rhok, NHP, NH, ts, 8, tw); break;
+            case 9: k_c2r_z_phi<R, K, N><<<zblocks(), nt, SM9, s>>>(rhok, phi, ts, wr, wt, tw, twh); break;
             default: break;
         }
     }
 
-    static void initial_density(cudaStream_t s, C *psi, C *rhok, TState *ts, const C *tw, const C *twh,
-                                double mu) {
-        k_density_r2c_z<R, N, false><<<zblocks(), TL::NT, SM, s>>>(psi, rhok, ts, mu, tw, twh);
+    static void initial_density(cudaStream_t s, G *psi, G *rhok, TState *ts, double *part, const C *tw,
+                                const C *twh) {
+        k_density_r2c_z<R, K, N, false><<<zblocks(), TL::NT, SM, s>>>(psi, rhok, ts, part, tw, twh);
+        k_reduce_init<<<1, 256, 0, s>>>(ts, part, (int)zblocks(), double(N) * N * N);
     }
 
-    static void fft3d(C *data, int sign, const C *tw, cudaStream_t s) {
+    static void fft3d(G *data, int sign, const C *tw, cudaStream_t s) {
         const unsigned nt = TL::NT;
         if (sign < 0) {
-            k_fft_z<R, N, -1><<<zblocks(), nt, SM, s>>>(data, tw);
-            k_fft_yx<R, N, -1, 1><<<zblocks(), nt, SM, s>>>(data, N, N, tw);
-            k_fft_yx<R, N, -1, 2><<<zblocks(), nt, SM, s>>>(data, N, N, tw);
+            k_fft_z<R, K, N, -1><<<zblocks(), nt, SM, s>>>(data, tw);
+            k_fft_yx<R, K, N, -1, 1><<<zblocks(), nt, SM, s>>>(data, N, N, nullptr, 0, tw);
+            k_fft_yx<R, K, N, -1, 2><<<zblocks(), nt, SM, s>>>(data, N, N, nullptr, 0, tw);
         } else {
-            k_fft_z<R, N, +1><<<zblocks(), nt, SM, s>>>(data, tw);
-            k_fft_yx<R, N, +1, 1><<<zblocks(), nt, SM, s>>>(data, N, N, tw);
-            k_fft_yx<R, N, +1, 2><<<zblocks(), nt, SM, s>>>(data, N, N, tw);
+            k_fft_z<R, K, N, +1><<<zblocks(), nt, SM, s>>>(data, tw);
+            k_fft_yx<R, K, N, +1, 1><<<zblocks(), nt, SM, s>>>(data, N, N, nullptr, 0, tw);
+            k_fft_yx<R, K, N, +1, 2><<<zblocks(), nt, SM, s>>>(data, N, N, nullptr, 0, tw);
         }
     }
 };
 
-// Runtime N -> Box<R, N>
-template <typename R, typename F> static std::string with_box(int n, F &&f) {
+// Runtime (N, precision) -> Box<R, K, N>
+template <typename R, typename K, typename F> static std::string with_box(int n, F &&f) {
     switch (n) {
-        case 16: return f(Box<R, 16>{});
-        case 32: return f(Box<R, 32>{});
-        case 48: return f(Box<R, 48>{});
-        case 64: return f(Box<R, 64>{});
-        case 96: return f(Box<R, 96>{});
-        case 128: return f(Box<R, 128>{});
-        case 256: return f(Box<R, 256>{});
-        case 512: return f(Box<R, 512>{});
+        case 16: return f(Box<R, K, 16>{});
+        case 32: return f(Box<R, K, 32>{});
+        case 48: return f(Box<R, K, 48>{});
+        case 64: return f(Box<R, K, 64>{});
+        case 96: return f(Box<R, K, 96>{});
+        case 128: return f(Box<R, K, 128>{});
+        case 256: return f(Box<R, K, 256>{});
+        case 512: return f(Box<R, K, 512>{});
         default: return "unsupported grid size " + std::to_string(n);
     }
 }
 template <typename F> static std::string with_box2(int n, int prec, F &&f) {
-    return prec == 0 ? with_box<double>(n, f) : with_box<float>(n, f);
+    switch (prec) {
+        case 0: return with_box<double, double>(n, f);
+        case 1: return with_box<float, float>(n, f);
+        case 2: return with_box<float, double>(n, f);
+        default: return "unknown precision " + std::to_string(prec);
+    }
 }
+// cuTensorMapEncodeTiled through the runtime's driver entry point (no libcuda link)
+static std::string encode_map(CUtensorMap *m, void *base, bool f64, int rank, const cuuint64_t *dims,
+                              const cuuint64_t *strides, const cuuint32_t *box) {
+    static PFN_cuTensorMapEncodeTiled_v12000 fn = nullptr;
+    if (!fn) {
+        cudaDriverEntryPointQueryResult q;
+        CUDA_TRY(cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", (void **)&fn, cudaEnableDefault, &q));
+        if (q != cudaDriverEntryPointSuccess || !fn) return "cuTensorMapEncodeTiled unavailable";
+    }
+    cuuint32_t estr[3] = {1, 1, 1};
+    CUresult r = fn(m, f64 ? CU_TENSOR_MAP_DATA_TYPE_FLOAT64 : CU_TENSOR_MAP_DATA_TYPE_FLOAT32, (cuuint32_t)rank,
+                    base, dims, strides, box, estr, CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE,
+                    CU_TENSOR_MAP_L2_PROMOTION_L2_256B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+    return r == CUDA_SUCCESS ? "" : "cuTensorMapEncodeTiled failed (" + std::to_string((int)r) + ")";
+}
+
+// y-pass map: [x][y][W complex] as (2W reals, N, N); x-pass map: (2*N*W reals, N)
+static std::string make_axis_maps(CUtensorMap *my, CUtensorMap *mx, void *base, bool f64, int N, int W, int L,
+                                  int boxr) {
+    const cuuint64_t es = f64 ? 8 : 4;
+    const cuuint64_t dy[3] = {cuuint64_t(2) * W, cuuint64_t(N), cuuint64_t(N)};
+    const cuuint64_t sy[2] = {cuuint64_t(2) * W * es, cuuint64_t(2) * W * N * es};
+    const cuuint32_t by[3] = {cuuint32_t(2 * L), cuuint32_t(boxr), 1};
+    std::string e = encode_map(my, base, f64, 3, dy, sy, by);
+    if (!e.empty()) return e;
+    const cuuint64_t dx[2] = {cuuint64_t(2) * N * W, cuuint64_t(N)};
+    const cuuint64_t sx[1] = {cuuint64_t(2) * W * N * es};
+    const cuuint32_t bx[2] = {cuuint32_t(2 * L), cuuint32_t(boxr)};
+    return encode_map(mx, base, f64, 2, dx, sx, bx);
+}
+
+// arithmetic type of a precision mode: 0 double, 1 float
+static int compute_kind(int prec) { return prec == 1 ? 1 : 0; }
+static size_t storage_bytes(int prec) { return prec == 0 ? 8 : 4; }
 
 // twiddles exp(-2 pi i m / n), m < n, from long double
 template <typename C> static std::vector<C> twiddles(int n) {
@@ -166,6 +241,7 @@ StepEngine::~StepEngine() {
     cudaFree(drift64_);
     cudaFree(drift32_);
     cudaFree(ts_);
+    cudaFree(part_);
 }
 
 std::string StepEngine::init(const EngineConfig &cfg, cudaStream_t stream) {
@@ -174,7 +250,7 @@ std::string StepEngine::init(const EngineConfig &cfg, cudaStream_t stream) {
     const int N = cfg.N;
     if (!supported_n(N)) return "unsupported grid size " + std::to_string(N);
     const size_t n3 = n3_();
-    const size_t cs = cfg.precision == 0 ? 16 : 8, rs = cs / 2;
+    const size_t rs = storage_bytes(cfg.precision), cs = 2 * rs;
     const int nhp = cfg.precision == 0 ? half_pitch<double>(N) : half_pitch<float>(N);
     CUDA_TRY(cudaMalloc(&psi_, n3 * cs));
     CUDA_TRY(cudaMalloc(&phi_, n3 * rs));
@@ -184,12 +260,27 @@ std::string StepEngine::init(const EngineConfig &cfg, cudaStream_t stream) {
     CUDA_TRY(cudaMalloc(&drift32_, sizeof(float2) * N));
     CUDA_TRY(cudaMalloc(&ts_, sizeof(TState)));
     CUDA_TRY(cudaMemsetAsync(ts_, 0, sizeof(TState), stream_));
-    std::string e = get_twiddles(N, cfg.precision, &tw_);
+    std::string e = get_twiddles(N, compute_kind(cfg.precision), &tw_);
     if (!e.empty()) return e;
-    e = get_twiddles(N / 2, cfg.precision, &twh_);
+    e = get_twiddles(N / 2, compute_kind(cfg.precision), &twh_);
     if (!e.empty()) return e;
     e = with_box2(N, cfg.precision, [](auto box) { return decltype(box)::configure(); });
     if (!e.empty()) return e;
+    // TMA descriptors for the pipelined y/x passes
+    use_tma_ = N >= 128 && cfg.precision != 2 && std::getenv("IFDM_NO_TMA") == nullptr;
+    if (use_tma_) {
+        const bool f64 = cfg.precision == 0;
+        const int L = f64 ? 8 : 16, boxr = N < 256 ? N : 256;
+        e = make_axis_maps(&map_psi_y_, &map_psi_x_, psi_, f64, N, N, L, boxr);
+        if (e.empty()) e = make_axis_maps(&map_rho_y_, &map_rho_x_, rhok_, f64, N, nhp, L, boxr);
+        if (!e.empty()) return e;
+        int dev = 0, sms = 0;
+        CUDA_TRY(cudaGetDevice(&dev));
+        CUDA_TRY(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));
+        const size_t tile = size_t(N) * L * (f64 ? 16 : 8);
+        const int per_sm = (3 * tile + 64) * 2 <= 227 * 1024 ? 2 : 1;
+        tma_grid_ = sms * per_sm;
+    }
     // max|phi| scan window of the reference: first N^3 doubles of the padded
     // [N][N][2(N/2+1)] array (the vector holds only N^3 elements,
     // src/struct3D.h:110,117; scanned at src/CosmoBEC_MPI.cpp:26)
@@ -208,7 +299,6 @@ std::string StepEngine::set_physics(double a, double rhoc) {
     const double m = cfg_.mfdm, ms = cfg_.mfdm_solar;
     const double S2 = rhoc / ms;
     S_ = std::sqrt(S2);
-    mu_ = 1.0;
     Phi0_ = 4.0 * M_PI * bigG * rhoc * (cfg_.xmax / M_PI) * (cfg_.xmax / M_PI);
     Phys &ph = phys_;
     ph.A_KE = 4. / (3. * M_PI) * (m / pow(c, 2)) / hbar * pow(cfg_.dx, 2);
@@ -242,6 +332,7 @@ std::string StepEngine::load_psi(const double *psi, bool on_device, double a, do
     if (on_device) {
         if (prec == 0) k_psi_in<double><<<1184, 256, 0, stream_>>>((const double2 *)psi, (double2 *)psi_, invS, n3);
         else k_psi_in<float><<<1184, 256, 0, stream_>>>((const double2 *)psi, (float2 *)psi_, invS, n3);
+
         CUDA_TRY(cudaGetLastError());
     } else {
         const size_t chunk = std::min<size_t>(n3, size_t(1) << 22);
@@ -263,16 +354,20 @@ std::string StepEngine::load_psi(const double *psi, bool on_device, double a, do
 }
 
 std::string StepEngine::launch_initial_density() {
-    const double mu = mu_;
     return with_box2(cfg_.N, cfg_.precision, [&](auto box) -> std::string {
         using B = decltype(box);
         using C = typename B::C;
-        using R = decltype(C{}.x);
-        C *psi = (C *)psi_, *rhok = (C *)rhok_;
+        using G = typename B::G;
+        using R = typename B::R;
+        G *psi = (G *)psi_, *rhok = (G *)rhok_;
         R *phi = (R *)phi_;
         const C *tw = (const C *)tw_, *twh = (const C *)twh_;
-        B::initial_density(stream_, psi, rhok, ts_, tw, twh, mu);
-        for (int p = 6; p <= 9; ++p) B::pass(p, stream_, psi, phi, rhok, ts_, nullptr, tw, twh, mu, win_rows_, win_tail_);
+        if (!part_) CUDA_TRY(cudaMalloc(&part_, sizeof(double) * 3 * B::zblocks()));
+        B::initial_density(stream_, psi, rhok, ts_, part_, tw, twh);
+        const CUtensorMap tm[4] = {map_psi_y_, map_psi_x_, map_rho_y_, map_rho_x_};
+        for (int p = 6; p <= 9; ++p)
+            B::pass(p, stream_, psi, phi, rhok, ts_, nullptr, tw, twh, win_rows_, win_tail_, use_tma_ ? tm : nullptr,
+                    tma_grid_);
         CUDA_TRY(cudaGetLastError());
         return "";
     });
@@ -288,17 +383,19 @@ std::string StepEngine::launch_timestep(double dt_scale) {
 }
 
 std::string StepEngine::launch_passes(cudaEvent_t *ev) {
-    const double mu = mu_;
     return with_box2(cfg_.N, cfg_.precision, [&](auto box) -> std::string {
         using B = decltype(box);
         using C = typename B::C;
-        using R = decltype(C{}.x);
-        C *psi = (C *)psi_, *rhok = (C *)rhok_;
+        using G = typename B::G;
+        using R = typename B::R;
+        G *psi = (G *)psi_, *rhok = (G *)rhok_;
         R *phi = (R *)phi_;
         const C *tw = (const C *)tw_, *twh = (const C *)twh_;
-        const C *drift = cfg_.precision == 0 ? (const C *)(void *)drift64_ : (const C *)(void *)drift32_;
+        const C *drift = compute_kind(cfg_.precision) == 0 ? (const C *)(void *)drift64_ : (const C *)(void *)drift32_;
+        const CUtensorMap tm[4] = {map_psi_y_, map_psi_x_, map_rho_y_, map_rho_x_};
         for (int p = 1; p <= 9; ++p) {
-            B::pass(p, stream_, psi, phi, rhok, ts_, drift, tw, twh, mu, win_rows_, win_tail_);
+            B::pass(p, stream_, psi, phi, rhok, ts_, drift, tw, twh, win_rows_, win_tail_, use_tma_ ? tm : nullptr,
+                    tma_grid_);
             if (ev) CUDA_TRY(cudaEventRecord(ev[p], stream_));
         }
         CUDA_TRY(cudaGetLastError());
@@ -349,7 +446,7 @@ std::vector<double> StepEngine::pass_bytes() const {
     const double n3 = (double)n3_();
     const double N = cfg_.N;
     const double nh = N * N * (N / 2 + 1);
-    const double cs = cfg_.precision == 0 ? 16 : 8, rs = cs / 2;
+    const double rs = (double)storage_bytes(cfg_.precision), cs = 2 * rs;
     return {0.0,
             n3 * (2 * cs + rs),         // P1 psi in/out + phi in
             2 * cs * n3,                // P2
@@ -393,14 +490,15 @@ std::string StepEngine::read_state(TState &out) {
 std::string fft3d(void *data, int n, int precision, int sign, cudaStream_t stream) {
     if (!supported_n(n)) return "unsupported grid size " + std::to_string(n);
     void *tw = nullptr;
-    std::string e = get_twiddles(n, precision, &tw);
+    std::string e = get_twiddles(n, compute_kind(precision), &tw);
     if (!e.empty()) return e;
     return with_box2(n, precision, [&](auto box) -> std::string {
         using B = decltype(box);
         using C = typename B::C;
+        using G = typename B::G;
         std::string e2 = B::configure();
         if (!e2.empty()) return e2;
-        B::fft3d((C *)data, sign, (const C *)tw, stream);
+        B::fft3d((G *)data, sign, (const C *)tw, stream);
         CUDA_TRY(cudaGetLastError());
         return "";
     });

@@ -1,6 +1,7 @@
 // step_engine.hpp -- device state and pass launcher of one simulation box.
 #pragma once
 
+#include <cuda.h>
 #include <cuda_runtime.h>
 
 #include "state_types.hpp"
@@ -72,9 +73,14 @@ class StepEngine {
     double2 *drift64_ = nullptr;
     float2 *drift32_ = nullptr;
     TState *ts_ = nullptr;
+    double *part_ = nullptr;  // per-block partial sums of the initial pass
     Phys phys_{};
-    double S_ = 1, Phi0_ = 1, mu_ = 1;
+    double S_ = 1, Phi0_ = 1;
     long win_rows_ = 0;
+    // TMA descriptors of the y/x passes (psi and the half spectrum), used for N >= 128
+    bool use_tma_ = false;
+    CUtensorMap map_psi_y_{}, map_psi_x_{}, map_rho_y_{}, map_rho_x_{};
+    int tma_grid_ = 0;
     int win_tail_ = 0;
 };
 

@@ -33,15 +33,28 @@
 namespace ifdm {
 
 // ------------------------------------------------------------ tile config --
-template <typename R, int N> struct Tile {
-    static constexpr int E = Plan<N>::E;
-    static constexpr int T = N / E;                              // threads per line
-    static constexpr int PH = sizeof(cx<R>) == 16 ? 8 : 16;      // threads per smem phase
-    static constexpr int LW = (256 / T > PH) ? 256 / T : PH;     // lines per tile
-    static constexpr int L = LW;
+// R: element type in HBM, K: arithmetic type in registers and shared memory.
+// (double, double) is the FP64 drop-in, (float, float) FP32, and
+// (float, double) the mixed mode: FP32 traffic, FP64 butterflies.
+template <typename R, typename K, int N> struct Tile {
+    using G = cx<R>;
+    using C = cx<K>;
+    static constexpr int GB = (int)sizeof(G);
+    static constexpr int PH = sizeof(C) == 16 ? 8 : 16;            // threads per smem phase
+    static constexpr int LC = 128 / GB;                             // lines for 128-byte rows
+    static constexpr int E0 = Plan<N>::E * ((sizeof(C) == 16 && GB == 8 && N >= 256) ? 2 : 1);
+    static constexpr int T = N / E0;                                // threads per line
+    static constexpr int LT = 256 / T;                              // lines for >= 256 threads
+    static constexpr int L1 = LT > LC ? LT : LC;
+    static constexpr int L = L1 > PH ? L1 : PH;                     // lines per tile
+    static constexpr int E = E0;
     static constexpr int LP = L + 1;
-    static constexpr int NT = L * T;                             // threads per block
-    static constexpr size_t SMEM = size_t(N) * LP * sizeof(cx<R>);
+    static constexpr int NT = L * T;                                // threads per block
+    static constexpr int EH = elems_for<N / 2, T>(0);               // half-length lines
+    static constexpr size_t SMEM = size_t(N) * LP * sizeof(C);
+    static constexpr size_t SMEM9 = size_t(N + 1) * LP * sizeof(C);
+    static_assert(N / E0 * E0 == N, "E must divide N");
+    static_assert((N / 2) / EH <= T, "half-length lines must fit the block");
 };
 
 // Half-spectrum row pitch: N/2+1 rounded up so rows start on 128-byte lines.
@@ -62,6 +75,69 @@ template <typename R> __device__ __forceinline__ R warp_max(R v) {
     return v;
 }
 
+// ------------------------------------------------------- storage rounding --
+// Mixed mode rounds FP64 results to FP32 stochastically: the magnitude is
+// rounded up with probability equal to the discarded fraction of an ulp.
+// Consecutive steps see nearly the same data, so round-to-nearest would
+// repeat the same errors every step and let them add up linearly; stochastic
+// rounding makes them independent (unbiased, growing like sqrt(steps)).
+__device__ __forceinline__ uint32_t mix32(uint32_t x) {
+    x ^= x >> 16;
+    x *= 0x7feb352du;
+    x ^= x >> 15;
+    x *= 0x846ca68bu;
+    x ^= x >> 16;
+    return x;
+}
+__device__ __forceinline__ float sr_to_float(double v, uint32_t r) {
+    long long b = __double_as_longlong(v);
+    b += (long long)(r >> 3);        // 29 random bits below float precision
+    b &= ~((1ll << 29) - 1);
+    return __double2float_rz(__longlong_as_double(b));
+}
+// salt: per step and pass; idx: element index
+__device__ __forceinline__ uint32_t sr_key(uint32_t salt, size_t idx) {
+    return mix32(salt ^ (uint32_t)idx ^ mix32((uint32_t)(idx >> 32) + 0x9e3779b9u));
+}
+template <typename R, typename K> struct Cvt {
+    __device__ __forceinline__ static cx<R> out(cx<K> v, uint32_t, size_t) { return v; }
+    __device__ __forceinline__ static R outr(K v, uint32_t, size_t) { return v; }
+};
+template <> struct Cvt<float, double> {
+    __device__ __forceinline__ static float2 out(double2 v, uint32_t salt, size_t idx) {
+        const uint32_t k = sr_key(salt, idx);
+        return make_float2(sr_to_float(v.x, k), sr_to_float(v.y, mix32(k ^ 0x5bd1e995u)));
+    }
+    __device__ __forceinline__ static float outr(double v, uint32_t salt, size_t idx) {
+        return sr_to_float(v, sr_key(salt, idx));
+    }
+};
+template <typename K, typename G> __device__ __forceinline__ cx<K> cin(G g) {
+    return mkc((K)g.x, (K)g.y);
+}
+__device__ __forceinline__ uint32_t pass_salt(const TState *ts, int pass) {
+    return mix32((uint32_t)ts->steps * 16u + (uint32_t)pass);
+}
+
+// Deterministic block sum of three doubles; thread 0 writes out[0..2].
+__device__ __forceinline__ void block_sum3(double a, double b, double c, double *out) {
+    __shared__ double red[3][32];
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) {
+        a += __shfl_xor_sync(0xffffffffu, a, o);
+        b += __shfl_xor_sync(0xffffffffu, b, o);
+        c += __shfl_xor_sync(0xffffffffu, c, o);
+    }
+    const int w = threadIdx.x >> 5, nw = (blockDim.x + 31) >> 5;
+    if ((threadIdx.x & 31) == 0) { red[0][w] = a; red[1][w] = b; red[2][w] = c; }
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        double s0 = 0, s1 = 0, s2 = 0;
+        for (int i = 0; i < nw; ++i) { s0 += red[0][i]; s1 += red[1][i]; s2 += red[2][i]; }
+        out[0] = s0; out[1] = s1; out[2] = s2;
+    }
+}
+
 // exp(-i p) for the kick; FP32 reduces the FP64 argument mod 2 pi first.
 template <typename R> __device__ __forceinline__ cx<R> expmi(double p);
 template <> __device__ __forceinline__ double2 expmi<double>(double p) {
@@ -80,48 +156,55 @@ template <> __device__ __forceinline__ float2 expmi<float>(double p) {
 // ------------------------------------------------------------- z-passes ---
 // Tiles of L consecutive rows (row r = x*N + y), row pitch N, contiguous.
 
-template <typename R, int N, int DIR>
-__global__ void __launch_bounds__(Tile<R, N>::NT) k_fft_z(cx<R> *__restrict__ data, const cx<R> *__restrict__ tw) {
-    using C = cx<R>;
-    using TL = Tile<R, N>;
+template <typename R, typename K, int N, int DIR>
+__global__ void __launch_bounds__(Tile<R, K, N>::NT)
+    k_fft_z(cx<R> *__restrict__ data, const cx<K> *__restrict__ tw) {
+    using TL = Tile<R, K, N>;
+    using C = typename TL::C;
     extern __shared__ __align__(16) unsigned char smraw[];
     C *sm = reinterpret_cast<C *>(smraw);
     const size_t base = size_t(blockIdx.x) * TL::L * N;
-    for (int f = threadIdx.x; f < TL::L * N; f += TL::NT) sm[(f % N) * TL::LP + f / N] = data[base + f];
+    for (int f = threadIdx.x; f < TL::L * N; f += TL::NT) sm[(f % N) * TL::LP + f / N] = cin<K>(data[base + f]);
     __syncthreads();
-    fft_tile<C, N, DIR, TL::L, TL::LP>(sm, tw);
-    for (int f = threadIdx.x; f < TL::L * N; f += TL::NT) data[base + f] = sm[(f % N) * TL::LP + f / N];
+    fft_tile<C, N, TL::E, DIR, TL::L, TL::LP>(sm, tw);
+    for (int f = threadIdx.x; f < TL::L * N; f += TL::NT)
+        data[base + f] = Cvt<R, K>::out(sm[(f % N) * TL::LP + f / N], 0x2545f491u, base + f);
 }
 
-// P1: kick with the merged coefficients, then forward FFT along z.
-template <typename R, int N>
-__global__ void __launch_bounds__(Tile<R, N>::NT)
+// P1: kick with the merged coefficients, remove the offset c, forward FFT along z.
+template <typename R, typename K, int N>
+__global__ void __launch_bounds__(Tile<R, K, N>::NT)
     k_kick_fft_z(cx<R> *__restrict__ psi, const R *__restrict__ phi, const TState *__restrict__ ts,
-                 const cx<R> *__restrict__ tw) {
-    using C = cx<R>;
-    using TL = Tile<R, N>;
+                 const cx<K> *__restrict__ tw) {
+    using TL = Tile<R, K, N>;
+    using C = typename TL::C;
     extern __shared__ __align__(16) unsigned char smraw[];
     C *sm = reinterpret_cast<C *>(smraw);
     const double cp = ts->coefP, cq = ts->coefQ;
+    const C c0 = mkc((K)ts->cre, (K)ts->cim);
+    const uint32_t salt = pass_salt(ts, 1);
     const size_t base = size_t(blockIdx.x) * TL::L * N;
     for (int f = threadIdx.x; f < TL::L * N; f += TL::NT) {
-        C v = psi[base + f];
+        const C v = cin<K>(psi[base + f]);
         const double p = cp * (double)phi[base + f] + cq * (double)cnorm2(v);
-        sm[(f % N) * TL::LP + f / N] = cmul(v, expmi<R>(p));
+        sm[(f % N) * TL::LP + f / N] = cmul(v, expmi<K>(p)) - c0;
     }
     __syncthreads();
-    fft_tile<C, N, -1, TL::L, TL::LP>(sm, tw);
-    for (int f = threadIdx.x; f < TL::L * N; f += TL::NT) psi[base + f] = sm[(f % N) * TL::LP + f / N];
+    fft_tile<C, N, TL::E, -1, TL::L, TL::LP>(sm, tw);
+    for (int f = threadIdx.x; f < TL::L * N; f += TL::NT)
+        psi[base + f] = Cvt<R, K>::out(sm[(f % N) * TL::LP + f / N], salt, base + f);
 }
 
-// P5 (DO_IFFT) / initial density (no IFFT): rho = |psi|^2 - mu, max |psi|^2,
-// real-to-half-complex FFT of rho along z into rhok (pitch NHP).
-template <typename R, int N, bool DO_IFFT>
-__global__ void __launch_bounds__(Tile<R, N>::NT)
-    k_density_r2c_z(cx<R> *__restrict__ psi, cx<R> *__restrict__ rhok, TState *__restrict__ ts, double mu,
-                    const cx<R> *__restrict__ tw, const cx<R> *__restrict__ twh) {
-    using C = cx<R>;
-    using TL = Tile<R, N>;
+// P5 (DO_IFFT) / initial density (no IFFT): psi = IFFT + c, rho = |psi|^2 - mu,
+// max |psi|^2, real-to-half-complex FFT of rho along z into rhok (pitch NHP).
+// The initial pass (no IFFT) also writes per-block partial sums of psi and
+// |psi|^2 to `part` (3 doubles per block) for the offset c and the mean mu.
+template <typename R, typename K, int N, bool DO_IFFT>
+__global__ void __launch_bounds__(Tile<R, K, N>::NT)
+    k_density_r2c_z(cx<R> *__restrict__ psi, cx<R> *__restrict__ rhok, TState *__restrict__ ts,
+                    double *__restrict__ part, const cx<K> *__restrict__ tw, const cx<K> *__restrict__ twh) {
+    using TL = Tile<R, K, N>;
+    using C = typename TL::C;
     constexpr int NH = N / 2 + 1;
     constexpr int NHP = half_pitch<R>(N);
     constexpr int M = N / 2;
@@ -129,33 +212,42 @@ __global__ void __launch_bounds__(Tile<R, N>::NT)
     C *sm = reinterpret_cast<C *>(smraw);
     const size_t row0 = size_t(blockIdx.x) * TL::L;
     const size_t base = row0 * N;
+    const uint32_t salt = pass_salt(ts, 5), salt2 = pass_salt(ts, 10);
     if (DO_IFFT) {
-        for (int f = threadIdx.x; f < TL::L * N; f += TL::NT) sm[(f % N) * TL::LP + f / N] = psi[base + f];
+        for (int f = threadIdx.x; f < TL::L * N; f += TL::NT) sm[(f % N) * TL::LP + f / N] = cin<K>(psi[base + f]);
         __syncthreads();
-        fft_tile<C, N, +1, TL::L, TL::LP>(sm, tw);
+        fft_tile<C, N, TL::E, +1, TL::L, TL::LP>(sm, tw);
     }
     // rho values: thread keeps its E elements (fixed stride NT over the tile)
-    R rho[TL::E];
+    K rho[TL::E];
     double mx = 0.0;
+    const double mu = DO_IFFT ? ts->mu : 0.0;
+    const C c0 = DO_IFFT ? mkc((K)ts->cre, (K)ts->cim) : mkc(K(0), K(0));
+    double sre = 0.0, sim = 0.0, sn2 = 0.0;
 #pragma unroll
     for (int i = 0; i < TL::E; ++i) {
         const int f = threadIdx.x + i * TL::NT;
         C v;
         if (DO_IFFT) {
-            v = sm[(f % N) * TL::LP + f / N];
-            psi[base + f] = v;
+            const typename TL::G g = Cvt<R, K>::out(sm[(f % N) * TL::LP + f / N] + c0, salt, base + f);
+            psi[base + f] = g;
+            v = cin<K>(g);  // the stored value defines the density
         } else {
-            v = psi[base + f];
+            v = cin<K>(psi[base + f]);
+            sre += (double)v.x;
+            sim += (double)v.y;
         }
         const double n2 = (double)cnorm2(v);
+        sn2 += n2;
         mx = fmax(mx, n2);
-        rho[i] = (R)(n2 - mu);
+        rho[i] = (K)(n2 - mu);
     }
     mx = warp_max(mx);
     if ((threadIdx.x & 31) == 0) atomic_max_nonneg(&ts->maxrho_bits, mx);
+    if (!DO_IFFT) block_sum3(sre, sim, sn2, part + 3 * blockIdx.x);
     __syncthreads();
     // pack z_m = rho_{2m} + i rho_{2m+1} into the half tile (rows m < N/2)
-    R *smr = reinterpret_cast<R *>(sm);
+    K *smr = reinterpret_cast<K *>(sm);
 #pragma unroll
     for (int i = 0; i < TL::E; ++i) {
         const int f = threadIdx.x + i * TL::NT;
@@ -163,40 +255,41 @@ __global__ void __launch_bounds__(Tile<R, N>::NT)
         smr[2 * ((n >> 1) * TL::LP + l) + (n & 1)] = rho[i];
     }
     __syncthreads();
-    fft_tile<C, M, -1, TL::L, TL::LP>(sm, twh);
+    fft_tile<C, M, TL::EH, -1, TL::L, TL::LP>(sm, twh);
     // X_k = (Z_k + conj Z_{M-k})/2 - i w^k (Z_k - conj Z_{M-k})/2, k = 0..M
     for (int f = threadIdx.x; f < TL::L * NH; f += TL::NT) {
         const int l = f / NH, k = f % NH;
         const C zk = sm[(k % M) * TL::LP + l];
         const C zc = cconj(sm[((M - k) % M) * TL::LP + l]);
-        const C e = cscale(zk + zc, R(0.5));
-        const C o = cscale(zk - zc, R(0.5));
+        const C e = cscale(zk + zc, K(0.5));
+        const C o = cscale(zk - zc, K(0.5));
         const C w = __ldg(tw + (k % N));
-        // -i * w * o
-        const C wo = cmul(w, o);
-        rhok[(row0 + l) * NHP + k] = mkc(e.x + wo.y, e.y - wo.x);
+        const C wo = cmul(w, o);  // X = e - i w o
+        const size_t gi = (row0 + l) * NHP + k;
+        rhok[gi] = Cvt<R, K>::out(mkc(e.x + wo.y, e.y - wo.x), salt2, gi);
     }
 }
 
 // P9: half-complex-to-real FFT along z, scale by 1/N^3, store phi, max|phi|
 // over the reference's scan window (rows below win_rows, plus win_tail
 // elements of row win_rows; see the timestep kernel).
-template <typename R, int N>
-__global__ void __launch_bounds__(Tile<R, N>::NT)
+template <typename R, typename K, int N>
+__global__ void __launch_bounds__(Tile<R, K, N>::NT)
     k_c2r_z_phi(const cx<R> *__restrict__ rhok, R *__restrict__ phi, TState *__restrict__ ts, long win_rows,
-                int win_tail, const cx<R> *__restrict__ tw, const cx<R> *__restrict__ twh) {
-    using C = cx<R>;
-    using TL = Tile<R, N>;
+                int win_tail, const cx<K> *__restrict__ tw, const cx<K> *__restrict__ twh) {
+    using TL = Tile<R, K, N>;
+    using C = typename TL::C;
     constexpr int NHP = half_pitch<R>(N);
     constexpr int M = N / 2;
     extern __shared__ __align__(16) unsigned char smraw[];
     C *sm = reinterpret_cast<C *>(smraw);
     C *xs = sm + M * TL::LP;  // X_k rows k = 0..M staged after the Z tile
     const size_t row0 = size_t(blockIdx.x) * TL::L;
+    const uint32_t salt = pass_salt(ts, 9);
     for (int f = threadIdx.x; f < TL::L * (M + 1); f += TL::NT) {
         const int l = f / (M + 1), k = f % (M + 1);
-        C x = rhok[(row0 + l) * NHP + k];
-        if (k == 0 || k == M) x.y = R(0);  // c2r ignores these imaginary parts
+        C x = cin<K>(rhok[(row0 + l) * NHP + k]);
+        if (k == 0 || k == M) x.y = K(0);  // c2r ignores these imaginary parts
         xs[k * TL::LP + l] = x;
     }
     __syncthreads();
@@ -210,13 +303,13 @@ __global__ void __launch_bounds__(Tile<R, N>::NT)
         sm[k * TL::LP + l] = mkc(e.x - d.y, e.y + d.x);
     }
     __syncthreads();
-    fft_tile<C, M, +1, TL::L, TL::LP>(sm, twh);
-    const R *smr = reinterpret_cast<const R *>(sm);
-    const R inv = R(1.0 / ((double)N * N * N));
+    fft_tile<C, M, TL::EH, +1, TL::L, TL::LP>(sm, twh);
+    const K *smr = reinterpret_cast<const K *>(sm);
+    const K inv = K(1.0 / ((double)N * N * N));
     double mx = 0.0;
     for (int f = threadIdx.x; f < TL::L * N; f += TL::NT) {
         const int l = f / N, n = f % N;
-        const R v = smr[2 * ((n >> 1) * TL::LP + l) + (n & 1)] * inv;
+        const R v = Cvt<R, K>::outr(smr[2 * ((n >> 1) * TL::LP + l) + (n & 1)] * inv, salt, row0 * N + f);
         phi[row0 * N + f] = v;
         const long row = (long)(row0 + l);
         if (row < win_rows || (row == win_rows && n < win_tail)) mx = fmax(mx, (double)fabs(v));
@@ -233,11 +326,12 @@ template <int AXIS> __device__ __forceinline__ size_t line_base(long g, int N, i
     return AXIS == 1 ? size_t(g / W) * N * W + (g % W) : size_t(g);
 }
 
-template <typename R, int N, int DIR, int AXIS>
-__global__ void __launch_bounds__(Tile<R, N>::NT)
-    k_fft_yx(cx<R> *__restrict__ data, int W, int VW, const cx<R> *__restrict__ tw) {
-    using C = cx<R>;
-    using TL = Tile<R, N>;
+template <typename R, typename K, int N, int DIR, int AXIS>
+__global__ void __launch_bounds__(Tile<R, K, N>::NT)
+    k_fft_yx(cx<R> *__restrict__ data, int W, int VW, const TState *__restrict__ ts, int pass,
+             const cx<K> *__restrict__ tw) {
+    using TL = Tile<R, K, N>;
+    using C = typename TL::C;
     extern __shared__ __align__(16) unsigned char smraw[];
     C *sm = reinterpret_cast<C *>(smraw);
     const int l = threadIdx.x % TL::L;
@@ -245,45 +339,58 @@ __global__ void __launch_bounds__(Tile<R, N>::NT)
     const bool valid = (g % W) < VW;
     const size_t b = line_base<AXIS>(g, N, W);
     const size_t S = AXIS == 1 ? size_t(W) : size_t(N) * W;
+    const uint32_t salt = ts ? pass_salt(ts, pass) : 0x9e3779b9u;
     for (int n = threadIdx.x / TL::L; n < N; n += TL::NT / TL::L)
-        sm[n * TL::LP + l] = valid ? data[b + n * S] : mkc(R(0), R(0));
+        sm[n * TL::LP + l] = valid ? cin<K>(data[b + n * S]) : mkc(K(0), K(0));
     __syncthreads();
-    fft_tile<C, N, DIR, TL::L, TL::LP>(sm, tw);
+    fft_tile<C, N, TL::E, DIR, TL::L, TL::LP>(sm, tw);
     if (valid)
-        for (int n = threadIdx.x / TL::L; n < N; n += TL::NT / TL::L) data[b + n * S] = sm[n * TL::LP + l];
+        for (int n = threadIdx.x / TL::L; n < N; n += TL::NT / TL::L)
+            data[b + n * S] = Cvt<R, K>::out(sm[n * TL::LP + l], salt, b + n * S);
 }
 
 // P3: x-pass forward, drift exp(-i s kappa^2) / N^3 from separable tables,
 // x-pass inverse.  drift[i] = exp(-i s kappa_i^2) written by the timestep.
-template <typename R, int N>
-__global__ void __launch_bounds__(Tile<R, N>::NT)
-    k_fft_x_drift(cx<R> *__restrict__ psi, const cx<R> *__restrict__ drift, const cx<R> *__restrict__ tw) {
-    using C = cx<R>;
-    using TL = Tile<R, N>;
+// The data are FFT(kicked psi - c); the drift leaves k = 0 unchanged, so c
+// is added back after the inverse z-pass (P5).
+template <typename R, typename K, int N>
+__global__ void __launch_bounds__(Tile<R, K, N>::NT)
+    k_fft_x_drift(cx<R> *__restrict__ psi, const cx<K> *__restrict__ drift, TState *__restrict__ ts,
+                  const cx<K> *__restrict__ tw) {
+    using TL = Tile<R, K, N>;
+    using C = typename TL::C;
     extern __shared__ __align__(16) unsigned char smraw[];
     C *sm = reinterpret_cast<C *>(smraw);
     const int l = threadIdx.x % TL::L;
     const long q = long(blockIdx.x) * TL::L + l;  // column = y*N + z
     const size_t S = size_t(N) * N;
-    for (int n = threadIdx.x / TL::L; n < N; n += TL::NT / TL::L) sm[n * TL::LP + l] = psi[q + n * S];
+    const uint32_t salt = pass_salt(ts, 3);
+    for (int n = threadIdx.x / TL::L; n < N; n += TL::NT / TL::L) sm[n * TL::LP + l] = cin<K>(psi[q + n * S]);
     __syncthreads();
-    fft_tile<C, N, -1, TL::L, TL::LP>(sm, tw);
+    fft_tile<C, N, TL::E, -1, TL::L, TL::LP>(sm, tw);
+    if (q == 0 && threadIdx.x == 0) {
+        // k = 0 coefficient = sum(kicked psi - c): the kicked field's mean, the next offset
+        const double inv = 1.0 / ((double)N * N * N);
+        ts->cnext_re = ts->cre + (double)sm[0].x * inv;
+        ts->cnext_im = ts->cim + (double)sm[0].y * inv;
+    }
     const int y = int(q / N), z = int(q % N);
-    const C lf = cscale(cmul(__ldg(drift + y), __ldg(drift + z)), R(1.0 / ((double)N * N * N)));
+    const C lf = cscale(cmul(__ldg(drift + y), __ldg(drift + z)), K(1.0 / ((double)N * N * N)));
     for (int n = threadIdx.x / TL::L; n < N; n += TL::NT / TL::L)
         sm[n * TL::LP + l] = cmul(sm[n * TL::LP + l], cmul(lf, __ldg(drift + n)));
     __syncthreads();
-    fft_tile<C, N, +1, TL::L, TL::LP>(sm, tw);
-    for (int n = threadIdx.x / TL::L; n < N; n += TL::NT / TL::L) psi[q + n * S] = sm[n * TL::LP + l];
+    fft_tile<C, N, TL::E, +1, TL::L, TL::LP>(sm, tw);
+    for (int n = threadIdx.x / TL::L; n < N; n += TL::NT / TL::L)
+        psi[q + n * S] = Cvt<R, K>::out(sm[n * TL::LP + l], salt, q + n * S);
 }
 
 // P7: x-pass forward on the half spectrum, multiply by -1/kappa^2 (0 at k=0),
 // x-pass inverse.
-template <typename R, int N>
-__global__ void __launch_bounds__(Tile<R, N>::NT)
-    k_fft_x_poisson(cx<R> *__restrict__ rhok, const cx<R> *__restrict__ tw) {
-    using C = cx<R>;
-    using TL = Tile<R, N>;
+template <typename R, typename K, int N>
+__global__ void __launch_bounds__(Tile<R, K, N>::NT)
+    k_fft_x_poisson(cx<R> *__restrict__ rhok, const TState *__restrict__ ts, const cx<K> *__restrict__ tw) {
+    using TL = Tile<R, K, N>;
+    using C = typename TL::C;
     constexpr int NH = N / 2 + 1;
     constexpr int NHP = half_pitch<R>(N);
     extern __shared__ __align__(16) unsigned char smraw[];
@@ -293,22 +400,24 @@ __global__ void __launch_bounds__(Tile<R, N>::NT)
     const int y = int(q / NHP), kz = int(q % NHP);
     const bool valid = kz < NH;
     const size_t S = size_t(N) * NHP;
+    const uint32_t salt = pass_salt(ts, 7);
     for (int n = threadIdx.x / TL::L; n < N; n += TL::NT / TL::L)
-        sm[n * TL::LP + l] = valid ? rhok[q + n * S] : mkc(R(0), R(0));
+        sm[n * TL::LP + l] = valid ? cin<K>(rhok[q + n * S]) : mkc(K(0), K(0));
     __syncthreads();
-    fft_tile<C, N, -1, TL::L, TL::LP>(sm, tw);
+    fft_tile<C, N, TL::E, -1, TL::L, TL::LP>(sm, tw);
     const int ky = kappa(y, N), kzz = kappa(kz, N);
     const int k2yz = ky * ky + kzz * kzz;
     for (int n = threadIdx.x / TL::L; n < N; n += TL::NT / TL::L) {
         const int kx = kappa(n, N);
         const int k2 = kx * kx + k2yz;
-        const R m = k2 == 0 ? R(0) : R(-1) / R(k2);
+        const K m = k2 == 0 ? K(0) : K(-1) / K(k2);
         sm[n * TL::LP + l] = cscale(sm[n * TL::LP + l], m);
     }
     __syncthreads();
-    fft_tile<C, N, +1, TL::L, TL::LP>(sm, tw);
+    fft_tile<C, N, TL::E, +1, TL::L, TL::LP>(sm, tw);
     if (valid)
-        for (int n = threadIdx.x / TL::L; n < N; n += TL::NT / TL::L) rhok[q + n * S] = sm[n * TL::LP + l];
+        for (int n = threadIdx.x / TL::L; n < N; n += TL::NT / TL::L)
+            rhok[q + n * S] = Cvt<R, K>::out(sm[n * TL::LP + l], salt, q + n * S);
 }
 
 // ------------------------------------------------------- state transfer ---

@@ -115,6 +115,35 @@ __device__ int qags_dev(int n, double H0, double Om, double a, double b, int lim
 
 __device__ __forceinline__ double bits_to_double(unsigned long long b) { return __longlong_as_double((long long)b); }
 
+// After the initial density pass: partial sums (3 per block, fixed order) ->
+// first offset c = mean psi_s and the conserved mean mu = <|psi_s|^2>.
+__global__ void k_reduce_init(TState *__restrict__ ts, const double *__restrict__ part, int nblocks, double n3) {
+    __shared__ double red[3][256];
+    double a = 0, b = 0, c = 0;
+    for (int i = threadIdx.x; i < nblocks; i += blockDim.x) {
+        a += part[3 * i];
+        b += part[3 * i + 1];
+        c += part[3 * i + 2];
+    }
+    red[0][threadIdx.x] = a;
+    red[1][threadIdx.x] = b;
+    red[2][threadIdx.x] = c;
+    __syncthreads();
+    for (int s = blockDim.x / 2; s > 0; s >>= 1) {
+        if ((int)threadIdx.x < s) {
+            red[0][threadIdx.x] += red[0][threadIdx.x + s];
+            red[1][threadIdx.x] += red[1][threadIdx.x + s];
+            red[2][threadIdx.x] += red[2][threadIdx.x + s];
+        }
+        __syncthreads();
+    }
+    if (threadIdx.x == 0) {
+        ts->cnext_re = red[0][0] / n3;
+        ts->cnext_im = red[1][0] / n3;
+        ts->mu = red[2][0] / n3;
+    }
+}
+
 // The timestep.  drift64/drift32: tables exp(-i s kappa_i^2), i < N.
 __global__ void k_timestep(TState *__restrict__ ts, Phys ph, double2 *__restrict__ drift64,
                            float2 *__restrict__ drift32) {
@@ -160,6 +189,8 @@ __global__ void k_timestep(TState *__restrict__ ts, Phys ph, double2 *__restrict
         ts->pendP = hp;
         ts->pendQ = hq;
         ts->drift_s = ph.kin * iKE;
+        ts->cre = ts->cnext_re;
+        ts->cim = ts->cnext_im;
         ts->steps += 1;
         s_drift = ph.kin * iKE;
     }

@@ -27,7 +27,8 @@ def _check(lib, h, rc: int) -> int:
 class Simulation:
     """One box on one GPU.
 
-    precision: "fp64" (the drop-in path) or "fp32" (FP32-mixed).
+    precision: "fp64" (the drop-in path), "fp32" (FP32 arithmetic) or "mixed"
+               (FP32 storage, FP64 arithmetic, stochastic FP32 rounding).
     ic_mode:   "ref1" reproduces the reference run on one MPI rank, "exact"
                deposits every IC particle once.
     """
@@ -42,7 +43,7 @@ class Simulation:
         p.mfdm, p.g, p.xmax, p.res = mfdm, g, xmax, res
         p.t_write, p.t_stop, p.ti = t_write, t_stop, ti
         p.opath, p.icpath, p.rerun = self._strs[0], self._strs[1], rerun
-        p.precision = {"fp64": _lib.FP64, "fp32": _lib.FP32}[precision]
+        p.precision = {"fp64": _lib.FP64, "fp32": _lib.FP32, "mixed": _lib.MIXED}[precision]
         p.stan = int(stan)
         p.ic_mode = {"ref1": _lib.IC_REF1, "exact": _lib.IC_EXACT}[ic_mode]
         p.device = device
@@ -135,9 +136,10 @@ class Simulation:
         return [b[i] for i in range(n)]
 
 
-def fft3d_(tensor, sign: int) -> None:
+def fft3d_(tensor, sign: int, compute: str | None = None) -> None:
     """In-place unnormalised 3-D FFT of a contiguous cubic CUDA complex tensor
-    (complex128 or complex64) on torch's current stream."""
+    (complex128 or complex64) on torch's current stream; compute="fp64" runs a
+    complex64 tensor through FP64 arithmetic."""
     import torch
 
     lib = _lib.load_library()
@@ -145,6 +147,8 @@ def fft3d_(tensor, sign: int) -> None:
         raise ValueError("need a contiguous 3-D CUDA tensor")
     n = tensor.shape[0]
     prec = {torch.complex128: _lib.FP64, torch.complex64: _lib.FP32}[tensor.dtype]
+    if compute == "fp64" and tensor.dtype == torch.complex64:
+        prec = _lib.MIXED
     stream = torch.cuda.current_stream(tensor.device).cuda_stream
     rc = lib.ifdm_fft3d(C.c_void_p(tensor.data_ptr()), n, prec, sign, C.c_void_p(stream))
     if rc < 0:
@@ -152,4 +156,4 @@ def fft3d_(tensor, sign: int) -> None:
 
 
 def supported_res(res: int, precision: str = "fp64") -> bool:
-    return bool(_lib.load_library().ifdm_supported_res(res, {"fp64": 0, "fp32": 1}[precision]))
+    return bool(_lib.load_library().ifdm_supported_res(res, {"fp64": 0, "fp32": 1, "mixed": 2}[precision]))

@@ -36,7 +36,14 @@ extern "C" {
 #define IFDM_ERR_STATE (-6)       /* call out of order (e.g. step before a psi exists) */
 #define IFDM_ERR_DEVICE (-7)      /* a device-side check failed (bounded wait, quadrature limit) */
 
-enum ifdm_precision { IFDM_FP64 = 0, IFDM_FP32 = 1 };
+/* FP64: complex128 state, FP64 arithmetic (the drop-in).
+ * FP32: complex64 state, FP32 FFTs/kick/drift; FP64 only for the phase
+ *       arguments (reduced mod 2 pi), twiddle generation, reductions and the
+ *       Poisson mean.
+ * MIXED: complex64 state in HBM, FP64 arithmetic inside every pass, FP32
+ *       stores rounded stochastically so rounding errors do not repeat
+ *       from step to step. */
+enum ifdm_precision { IFDM_FP64 = 0, IFDM_FP32 = 1, IFDM_MIXED = 2 };
 /* IC deposit: REF1 reproduces the reference run on one MPI rank (particles in
  * the last half cell deposited twice, one zero particle per chunk at the
  * origin: src/gadget_IC.h:431-448,496-510); EXACT deposits each particle once
@@ -57,7 +64,7 @@ typedef struct ifdm_params {
     const char *opath; /* output prefix (trailing '/')            argv[8] */
     const char *icpath;/* IC prefix, or snapshot dir when rerun   argv[9] */
     int rerun;         /* 1: start from <icpath>output<ti>.dat    argv[10] */
-    int precision;     /* IFDM_FP64 (drop-in) or IFDM_FP32 (mixed) */
+    int precision;     /* enum ifdm_precision; IFDM_FP64 is the drop-in */
     int stan;          /* 1: snapshot state machine of src/CosmoBEC_MPI_stan.cpp */
     int ic_mode;       /* enum ifdm_ic_mode */
     int device;        /* CUDA device ordinal */
@@ -131,7 +138,8 @@ int ifdm_pass_bytes(ifdm_ctx *ctx, double *bytes_out, int cap);
 
 /* Device-pointer transforms on the caller's stream (cudaStream_t as void*).
  * In-place unnormalised 3-D complex FFT of data[n][n][n] (complex128 when
- * precision == IFDM_FP64, complex64 otherwise); sign -1 forward, +1 backward
+ * precision == IFDM_FP64, complex64 otherwise; IFDM_MIXED computes in FP64);
+ * sign -1 forward, +1 backward
  * -- the contract of the reference's fftw_mpi_plan_dft_3d plans
  * (src/CosmoBEC_MPI.cpp:176-177). */
 int ifdm_fft3d(void *data, int n, int precision, int sign, void *stream);

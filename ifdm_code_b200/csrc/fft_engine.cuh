@@ -43,17 +43,19 @@ template <typename C> __device__ __forceinline__ auto cnorm2(C a) { return a.x *
 
 // ------------------------------------------------------------- radix plans --
 // Radix sequence per transform length; every radix divides E (elements per
-// thread), so a stage is E/R whole butterflies per thread.
+// thread), so a stage is E/R whole butterflies per thread.  Where possible the
+// first and last radix are equal: the last stage then leaves each thread
+// holding exactly the elements the first stage of the next transform reads.
 template <int N> struct Plan;
 template <> struct Plan<8> { static constexpr int E = 8, NST = 1; static constexpr int R[1] = {8}; };
 template <> struct Plan<16> { static constexpr int E = 8, NST = 2; static constexpr int R[2] = {8, 2}; };
 template <> struct Plan<24> { static constexpr int E = 12, NST = 3; static constexpr int R[3] = {4, 3, 2}; };
 template <> struct Plan<32> { static constexpr int E = 8, NST = 2; static constexpr int R[2] = {8, 4}; };
-template <> struct Plan<48> { static constexpr int E = 12, NST = 3; static constexpr int R[3] = {4, 4, 3}; };
+template <> struct Plan<48> { static constexpr int E = 12, NST = 3; static constexpr int R[3] = {4, 3, 4}; };
 template <> struct Plan<64> { static constexpr int E = 8, NST = 2; static constexpr int R[2] = {8, 8}; };
-template <> struct Plan<96> { static constexpr int E = 12, NST = 4; static constexpr int R[4] = {4, 4, 3, 2}; };
-template <> struct Plan<128> { static constexpr int E = 8, NST = 3; static constexpr int R[3] = {8, 8, 2}; };
-template <> struct Plan<256> { static constexpr int E = 8, NST = 3; static constexpr int R[3] = {8, 8, 4}; };
+template <> struct Plan<96> { static constexpr int E = 12, NST = 4; static constexpr int R[4] = {4, 3, 2, 4}; };
+template <> struct Plan<128> { static constexpr int E = 8, NST = 3; static constexpr int R[3] = {8, 2, 8}; };
+template <> struct Plan<256> { static constexpr int E = 8, NST = 3; static constexpr int R[3] = {8, 4, 8}; };
 template <> struct Plan<512> { static constexpr int E = 8, NST = 3; static constexpr int R[3] = {8, 8, 8}; };
 
 // ------------------------------------------------------------- butterflies --
@@ -198,6 +200,92 @@ __device__ __forceinline__ void fft_tile(C *sm, const C *__restrict__ tw) {
     const int l = tid % L;
     const int t = tid / L;
     StageLoop<C, N, E, DIR, L, LP, 0, 1>::run(sm, tw, l, t, t < T);
+}
+
+// ------------------------------------------------ register-resident chain --
+// The same Stockham stages with the stage inputs held in registers v[E]:
+// v[b*RAD + r] is element j + r*N/RAD of line l, j = t + T*b.
+
+template <typename C, int N, int E, int L, int LP, int RAD, typename SrcT>
+__device__ __forceinline__ void stage_load(const SrcT *src, C *v, int l, int t) {
+    constexpr int T = N / E, NB = E / RAD, STRIDE = N / RAD;
+#pragma unroll
+    for (int b = 0; b < NB; ++b)
+#pragma unroll
+        for (int r = 0; r < RAD; ++r) {
+            const auto g = src[(t + T * b + r * STRIDE) * LP + l];
+            v[b * RAD + r] = mkc((decltype(v[0].x))g.x, (decltype(v[0].x))g.y);
+        }
+}
+
+template <typename C, int N, int E, int DIR, int RAD, int NS>
+__device__ __forceinline__ void stage_compute(C *v, const C *__restrict__ tw, int t) {
+    constexpr int T = N / E, NB = E / RAD, TWSTEP = N / (NS * RAD);
+#pragma unroll
+    for (int b = 0; b < NB; ++b) {
+        const int k = (t + T * b) % NS;
+        if (NS > 1) {
+#pragma unroll
+            for (int r = 1; r < RAD; ++r) v[b * RAD + r] = cmul(v[b * RAD + r], twiddle<DIR>(tw, k * r * TWSTEP));
+        }
+        Bfly<RAD, DIR>::run(&v[b * RAD]);
+    }
+}
+
+template <typename C, int N, int E, int L, int LP, int RAD, int NS>
+__device__ __forceinline__ void stage_store(C *dst, const C *v, int l, int t) {
+    constexpr int T = N / E, NB = E / RAD;
+#pragma unroll
+    for (int b = 0; b < NB; ++b) {
+        const int j = t + T * b;
+        const int base = (j / NS) * NS * RAD + j % NS;
+#pragma unroll
+        for (int r = 0; r < RAD; ++r) dst[(base + r * NS) * LP + l] = v[b * RAD + r];
+    }
+}
+
+// Stages S.. of a transform whose stage S-1 outputs are in v: round trip
+// through `work` (barrier, store, barrier, load) then compute stage S.
+template <typename C, int N, int E, int DIR, int L, int LP, int S, int NS>
+struct RegChain {
+    __device__ __forceinline__ static void run(C *work, C *v, const C *__restrict__ tw, int l, int t, bool active) {
+        if constexpr (S < Plan<N>::NST) {
+            constexpr int RP = Plan<N>::R[S - 1];
+            constexpr int RAD = Plan<N>::R[S];
+            __syncthreads();
+            if (active) stage_store<C, N, E, L, LP, RP, NS / RP>(work, v, l, t);
+            __syncthreads();
+            if (active) {
+                stage_load<C, N, E, L, LP, RAD>(work, v, l, t);
+                stage_compute<C, N, E, DIR, RAD, NS>(v, tw, t);
+            }
+            RegChain<C, N, E, DIR, L, LP, S + 1, NS * RAD>::run(work, v, tw, l, t, active);
+        }
+    }
+};
+
+// Full transform: stage 0 reads `src` (any element type), later stages go
+// through `work`; on return v holds the outputs, v[b*R + r] = element
+// j + r*N/R (R the last radix, j = t + T*b).  `src` may alias `work`.
+template <typename C, int N, int E, int DIR, int L, int LP, typename SrcT>
+__device__ __forceinline__ void fft_regs(const SrcT *src, C *work, C *v, const C *__restrict__ tw, int l, int t,
+                                         bool active) {
+    constexpr int R0 = Plan<N>::R[0];
+    if (active) {
+        stage_load<C, N, E, L, LP, R0>(src, v, l, t);
+        stage_compute<C, N, E, DIR, R0, 1>(v, tw, t);
+    }
+    RegChain<C, N, E, DIR, L, LP, 1, R0>::run(work, v, tw, l, t, active);
+}
+
+// Second transform straight from the registers of a first one (requires the
+// plan's first and last radix to be equal).
+template <typename C, int N, int E, int DIR, int L, int LP>
+__device__ __forceinline__ void fft_regs_chained(C *work, C *v, const C *__restrict__ tw, int l, int t, bool active) {
+    constexpr int R0 = Plan<N>::R[0];
+    static_assert(Plan<N>::R[0] == Plan<N>::R[Plan<N>::NST - 1], "chained transform needs equal first/last radix");
+    if (active) stage_compute<C, N, E, DIR, R0, 1>(v, tw, t);
+    RegChain<C, N, E, DIR, L, LP, 1, R0>::run(work, v, tw, l, t, active);
 }
 
 }  // namespace ifdm

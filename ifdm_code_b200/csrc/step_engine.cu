@@ -70,18 +70,18 @@ template <typename R_, typename K_, int N> struct Box {
         CUDA_TRY(prep(k_fft_z<R, K, N, -1>, SM));
         CUDA_TRY(prep(k_fft_z<R, K, N, +1>, SM));
         if constexpr (kTma) {
-            CUDA_TRY(prep(k_yx_tma<R, N, 1, 0, -1>, TT::SMEM));
-            CUDA_TRY(prep(k_yx_tma<R, N, 1, 0, +1>, TT::SMEM));
-            CUDA_TRY(prep(k_yx_tma<R, N, 2, 1, 0>, TT::SMEM));
-            CUDA_TRY(prep(k_yx_tma<R, N, 2, 2, 0>, TT::SMEM));
+            CUDA_TRY(prep(k_yx_tma<R, K, N, 1, 0, -1>, TT::SMEM));
+            CUDA_TRY(prep(k_yx_tma<R, K, N, 1, 0, +1>, TT::SMEM));
+            CUDA_TRY(prep(k_yx_tma<R, K, N, 2, 1, 0>, TT::SMEM));
+            CUDA_TRY(prep(k_yx_tma<R, K, N, 2, 2, 0>, TT::SMEM));
         }
         done = true;
         return "";
     }
 
-    // TMA-pipelined y/x passes: FP32 and FP64 modes (R == K), N >= 128
-    static constexpr bool kTma = std::is_same<R, K>::value && N >= 128;
-    using TT = TmaTile<R, N>;
+    // TMA-pipelined y/x passes for N >= 128
+    static constexpr bool kTma = N >= 128;
+    using TT = TmaTile<R, K, N>;
 
     static unsigned zblocks() { return unsigned(size_t(N) * N / TL::L); }
     static unsigned hblocks() { return unsigned(size_t(N) * NHP / TL::L); }
@@ -95,14 +95,13 @@ template <typename R_, typename K_, int N> struct Box {
                 const int tc = int(size_t(N) * N / TT::L), th = int(size_t(N) * NHP / TT::L);
                 const unsigned g2 = unsigned(grid), tn = TT::NT;
                 const size_t sm = TT::SMEM;
-                const G *dG = reinterpret_cast<const G *>(drift);
                 switch (p) {
-                    case 2: k_yx_tma<R, N, 1, 0, -1><<<g2, tn, sm, s>>>(tm[0], psi, N, N, tc, ts, 2, dG, tw); break;
-                    case 3: k_yx_tma<R, N, 2, 1, 0><<<g2, tn, sm, s>>>(tm[1], psi, N, N, tc, ts, 3, dG, tw); break;
-                    case 4: k_yx_tma<R, N, 1, 0, +1><<<g2, tn, sm, s>>>(tm[0], psi, N, N, tc, ts, 4, dG, tw); break;
-                    case 6: k_yx_tma<R, N, 1, 0, -1><<<g2, tn, sm, s>>>(tm[2], rhok, NHP, NH, th, ts, 6, dG, tw); break;
-                    case 7: k_yx_tma<R, N, 2, 2, 0><<<g2, tn, sm, s>>>(tm[3], rhok, NHP, NH, th, ts, 7, dG, tw); break;
-                    case 8: k_yx_tma<R, N, 1, 0, +1><<<g2, tn, sm, s>>>(tm[2], rhok, NHP, NH, th, ts, 8, dG, tw); break;
+                    case 2: k_yx_tma<R, K, N, 1, 0, -1><<<g2, tn, sm, s>>>(tm[0], psi, N, N, tc, ts, 2, drift, tw); break;
+                    case 3: k_yx_tma<R, K, N, 2, 1, 0><<<g2, tn, sm, s>>>(tm[1], psi, N, N, tc, ts, 3, drift, tw); break;
+                    case 4: k_yx_tma<R, K, N, 1, 0, +1><<<g2, tn, sm, s>>>(tm[0], psi, N, N, tc, ts, 4, drift, tw); break;
+                    case 6: k_yx_tma<R, K, N, 1, 0, -1><<<g2, tn, sm, s>>>(tm[2], rhok, NHP, NH, th, ts, 6, drift, tw); break;
+                    case 7: k_yx_tma<R, K, N, 2, 2, 0><<<g2, tn, sm, s>>>(tm[3], rhok, NHP, NH, th, ts, 7, drift, tw); break;
+                    case 8: k_yx_tma<R, K, N, 1, 0, +1><<<g2, tn, sm, s>>>(tm[2], rhok, NHP, NH, th, ts, 8, drift, tw); break;
                 }
                 return;
             }
@@ -267,10 +266,10 @@ std::string StepEngine::init(const EngineConfig &cfg, cudaStream_t stream) {
     e = with_box2(N, cfg.precision, [](auto box) { return decltype(box)::configure(); });
     if (!e.empty()) return e;
     // TMA descriptors for the pipelined y/x passes
-    use_tma_ = N >= 128 && cfg.precision != 2 && std::getenv("IFDM_NO_TMA") == nullptr;
+    use_tma_ = N >= 128 && std::getenv("IFDM_NO_TMA") == nullptr;
     if (use_tma_) {
         const bool f64 = cfg.precision == 0;
-        const int L = f64 ? 8 : 16, boxr = N < 256 ? N : 256;
+        const int L = cfg.precision == 1 ? 16 : 8, boxr = N < 256 ? N : 256;
         e = make_axis_maps(&map_psi_y_, &map_psi_x_, psi_, f64, N, N, L, boxr);
         if (e.empty()) e = make_axis_maps(&map_rho_y_, &map_rho_x_, rhok_, f64, N, nhp, L, boxr);
         if (!e.empty()) return e;
@@ -278,7 +277,8 @@ std::string StepEngine::init(const EngineConfig &cfg, cudaStream_t stream) {
         CUDA_TRY(cudaGetDevice(&dev));
         CUDA_TRY(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));
         const size_t tile = size_t(N) * L * (f64 ? 16 : 8);
-        const int per_sm = (3 * tile + 64) * 2 <= 227 * 1024 ? 2 : 1;
+        const size_t work = cfg.precision == 2 ? size_t(N) * L * 16 : 0;
+        const int per_sm = (3 * tile + work + 64) * 2 <= 227 * 1024 ? 2 : 1;
         tma_grid_ = sms * per_sm;
     }
     // max|phi| scan window of the reference: first N^3 doubles of the padded

@@ -16,31 +16,42 @@
 #include "step_kernels.cuh"
 #include "tma.cuh"
 
+#include <type_traits>
+
 namespace ifdm {
 
-template <typename R, int N> struct TmaTile {
-    using C = cx<R>;
-    static constexpr int L = 128 / (int)sizeof(C);   // 8 complex doubles or 16 complex floats
+// R: element type in HBM (TMA landing ring), K: arithmetic type.  When they
+// differ (mixed mode) the landing slot is converted into a separate FP64
+// compute tile and freed before the transform; rows are then 64 bytes.
+template <typename R, typename K, int N> struct TmaTile {
+    using G = cx<R>;
+    using C = cx<K>;
+    static constexpr bool SPLIT = !std::is_same<R, K>::value;
+    static constexpr int L = SPLIT ? 8 : 128 / (int)sizeof(G);  // lines per tile
     static constexpr int E = Plan<N>::E;
     static constexpr int T = N / E;
     static constexpr int NT = L * T;
     static constexpr int STAGES = 3;
-    static constexpr int BOXR = N < 256 ? N : 256;    // rows per TMA box (limit 256)
-    static constexpr size_t TILE_BYTES = size_t(N) * L * sizeof(C);
-    static constexpr size_t SMEM = STAGES * TILE_BYTES + 64;
+    static constexpr int BOXR = N < 256 ? N : 256;               // rows per TMA box (limit 256)
+    static constexpr size_t TILE_BYTES = size_t(N) * L * sizeof(G);
+    static constexpr size_t WORK_BYTES = SPLIT ? size_t(N) * L * sizeof(C) : 0;
+    static constexpr size_t SMEM = STAGES * TILE_BYTES + WORK_BYTES + 64;
     static_assert(NT <= 1024, "block size");
+    static_assert(SMEM <= 227 * 1024, "shared memory per block");
 };
 
-template <typename R, int N, int AXIS, int MODE, int DIR>
-__global__ void __launch_bounds__(TmaTile<R, N>::NT, 1)
+template <typename R, typename K, int N, int AXIS, int MODE, int DIR>
+__global__ void __launch_bounds__(TmaTile<R, K, N>::NT, 1)
     k_yx_tma(const __grid_constant__ CUtensorMap map, cx<R> *__restrict__ data, int W, int VW, int ntiles,
-             TState *__restrict__ ts, int pass, const cx<R> *__restrict__ drift, const cx<R> *__restrict__ tw) {
-    using TL = TmaTile<R, N>;
-    using C = cx<R>;
+             TState *__restrict__ ts, int pass, const cx<K> *__restrict__ drift, const cx<K> *__restrict__ tw) {
+    using TL = TmaTile<R, K, N>;
+    using G = cx<R>;
+    using C = cx<K>;
     constexpr int L = TL::L, T = TL::T, ST = TL::STAGES;
     extern __shared__ __align__(128) unsigned char smraw[];
-    C *bufs = reinterpret_cast<C *>(smraw);
-    uint64_t *bar = reinterpret_cast<uint64_t *>(smraw + ST * TL::TILE_BYTES);
+    G *bufs = reinterpret_cast<G *>(smraw);
+    C *work = reinterpret_cast<C *>(smraw + ST * TL::TILE_BYTES);
+    uint64_t *bar = reinterpret_cast<uint64_t *>(smraw + ST * TL::TILE_BYTES + TL::WORK_BYTES);
     const int tid = threadIdx.x;
     const int l = tid % L;
     int *err = ts ? &ts->err : nullptr;
@@ -54,7 +65,7 @@ __global__ void __launch_bounds__(TmaTile<R, N>::NT, 1)
     auto issue = [&](int i) {
         const long t = (long)blockIdx.x + (long)i * gridDim.x;
         const int s = i % ST;
-        C *dst = bufs + (size_t)s * N * L;
+        G *dst = bufs + (size_t)s * N * L;
         const long g0 = t * L;
         mbar_arrive_expect_tx(&bar[s], (uint32_t)TL::TILE_BYTES);
 #pragma unroll
@@ -65,7 +76,7 @@ __global__ void __launch_bounds__(TmaTile<R, N>::NT, 1)
     };
     if (tid == 0)
         for (int i = 0; i < ST - 1 && i < my_n; ++i) issue(i);
-    (void)pass;
+    const uint32_t salt = ts ? pass_salt(ts, pass) : 0x2545f491u;
     const size_t S = AXIS == 1 ? size_t(W) : size_t(N) * W;
     for (int i = 0; i < my_n; ++i) {
         const int s = i % ST;
@@ -79,37 +90,60 @@ __global__ void __launch_bounds__(TmaTile<R, N>::NT, 1)
             __syncthreads();
             return;
         }
-        C *sm = bufs + (size_t)s * N * L;
         const long g = ((long)blockIdx.x + (long)i * gridDim.x) * L + l;
-        if (MODE == 0) {
-            fft_tile<C, N, TL::E, DIR, L, L>(sm, tw);
-        } else {
-            fft_tile<C, N, TL::E, -1, L, L>(sm, tw);
+        const int t = tid / L;
+        constexpr int R0 = Plan<N>::R[0];
+        constexpr int RL = Plan<N>::R[Plan<N>::NST - 1];
+        constexpr int E = TL::E;
+        C v[E];
+        const G *land = bufs + (size_t)s * N * L;
+        C *wk = TL::SPLIT ? work : reinterpret_cast<C *>(bufs + (size_t)s * N * L);
+        // stage 0 straight from the landing slot
+        stage_load<C, N, E, L, L, R0>(land, v, l, t);
+        if constexpr (TL::SPLIT) fence_proxy_async_smem();  // slot is released at the next barrier
+        stage_compute<C, N, E, (MODE == 0 ? DIR : -1), R0, 1>(v, tw, t);
+        RegChain<C, N, E, (MODE == 0 ? DIR : -1), L, L, 1, R0>::run(wk, v, tw, l, t, true);
+        if (MODE != 0) {
+            // v[b*RL + r] holds element n = (t + T*b) + r*N/RL of the forward transform
             if (MODE == 1) {
                 if (g == 0 && tid == 0) {
                     const double inv = 1.0 / ((double)N * N * N);
-                    ts->cnext_re = ts->cre + (double)sm[0].x * inv;
-                    ts->cnext_im = ts->cim + (double)sm[0].y * inv;
+                    ts->cnext_re = ts->cre + (double)v[0].x * inv;
+                    ts->cnext_im = ts->cim + (double)v[0].y * inv;
                 }
                 const int y = int(g / N), z = int(g % N);
-                const C lf = cscale(cmul(__ldg(drift + y), __ldg(drift + z)), R(1.0 / ((double)N * N * N)));
-                for (int n = tid / L; n < N; n += T) sm[n * L + l] = cmul(sm[n * L + l], cmul(lf, __ldg(drift + n)));
+                const C lf = cscale(cmul(__ldg(drift + y), __ldg(drift + z)), K(1.0 / ((double)N * N * N)));
+#pragma unroll
+                for (int b = 0; b < E / RL; ++b)
+#pragma unroll
+                    for (int r = 0; r < RL; ++r) {
+                        const int n = t + T * b + r * (N / RL);
+                        v[b * RL + r] = cmul(v[b * RL + r], cmul(lf, __ldg(drift + n)));
+                    }
             } else {
                 const int y = int(g / W), kz = int(g % W);
                 const int ky = kappa(y, N), kzz = kappa(kz, N);
                 const int k2yz = ky * ky + kzz * kzz;
-                for (int n = tid / L; n < N; n += T) {
-                    const int kx = kappa(n, N);
-                    const int k2 = kx * kx + k2yz;
-                    sm[n * L + l] = cscale(sm[n * L + l], k2 == 0 ? R(0) : R(-1) / R(k2));
-                }
+#pragma unroll
+                for (int b = 0; b < E / RL; ++b)
+#pragma unroll
+                    for (int r = 0; r < RL; ++r) {
+                        const int kx = kappa(t + T * b + r * (N / RL), N);
+                        const int k2 = kx * kx + k2yz;
+                        v[b * RL + r] = cscale(v[b * RL + r], k2 == 0 ? K(0) : K(-1) / K(k2));
+                    }
             }
-            __syncthreads();
-            fft_tile<C, N, TL::E, +1, L, L>(sm, tw);
+            fft_regs_chained<C, N, E, +1, L, L>(wk, v, tw, l, t, true);
         }
         if ((g % W) < VW) {
-            const size_t b = AXIS == 1 ? size_t(g / W) * N * W + size_t(g % W) : size_t(g);
-            for (int n = tid / L; n < N; n += T) data[b + n * S] = sm[n * L + l];
+            const size_t b0 = AXIS == 1 ? size_t(g / W) * N * W + size_t(g % W) : size_t(g);
+#pragma unroll
+            for (int b = 0; b < E / RL; ++b)
+#pragma unroll
+                for (int r = 0; r < RL; ++r) {
+                    const size_t gi = b0 + size_t(t + T * b + r * (N / RL)) * S;
+                    data[gi] = Cvt<R, K>::out(v[b * RL + r], salt, gi);
+                }
         }
         fence_proxy_async_smem();
         __syncthreads();

@@ -223,9 +223,10 @@ def test_fixed_steps_128_vs_oracle(ic128, tmp_path):
         assert s.state()["device_error"] == 0
 
 
-@pytest.mark.parametrize("prec", ["fp32", "fp64"])
+@pytest.mark.parametrize("prec", ["fp32", "fp64", "mixed"])
 def test_tma_passes_match_plain_passes(ic128, tmp_path, prec, monkeypatch):
-    """The TMA pipeline performs the same arithmetic as the plain passes."""
+    """The TMA pipeline computes the same transform as the plain passes (equal
+    up to floating-point contraction differences between the two kernels)."""
     out = {}
     for tma in (True, False):
         if tma:
@@ -236,4 +237,4 @@ def test_tma_passes_match_plain_passes(ic128, tmp_path, prec, monkeypatch):
             s.load_ic()
             s.step(5, 0.22)
             out[tma] = s.get_psi()
-    assert np.array_equal(out[True], out[False])
+    assert rel_l2(out[True], out[False]) <= (1e-13 if prec == "fp64" else 2e-6)

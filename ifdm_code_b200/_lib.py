@@ -27,7 +27,7 @@ EXPORTS = [
     "ifdm_params_default", "ifdm_params_from_argv", "ifdm_create", "ifdm_destroy", "ifdm_last_error",
     "ifdm_supported_res", "ifdm_load_ic", "ifdm_load_snapshot", "ifdm_set_psi", "ifdm_get_psi", "ifdm_get_phi",
     "ifdm_get_state", "ifdm_run", "ifdm_step", "ifdm_write_snapshot", "ifdm_synchronize", "ifdm_stream",
-    "ifdm_profile_passes", "ifdm_pass_bytes", "ifdm_fft3d",
+    "ifdm_profile_passes", "ifdm_pass_bytes", "ifdm_fft3d", "ifdm_poisson_static",
 ]
 
 
@@ -91,6 +91,7 @@ def load_library() -> C.CDLL:
     lib.ifdm_profile_passes.argtypes = [P, C.c_int, C.c_double, D, C.POINTER(C.c_char_p), C.c_int]
     lib.ifdm_pass_bytes.argtypes = [P, D, C.c_int]
     lib.ifdm_fft3d.argtypes = [C.c_void_p, C.c_int, C.c_int, C.c_int, C.c_void_p]
+    lib.ifdm_poisson_static.argtypes = [C.c_void_p, C.c_void_p, C.c_int, C.c_double, C.c_double, C.c_void_p]
     for name in EXPORTS:
         getattr(lib, name)  # raises AttributeError if an export is missing
     _lib = lib

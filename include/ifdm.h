@@ -144,6 +144,26 @@ int ifdm_pass_bytes(ifdm_ctx *ctx, double *bytes_out, int cap);
  * (src/CosmoBEC_MPI.cpp:176-177). */
 int ifdm_fft3d(void *data, int n, int precision, int sign, void *stream);
 
+/* Gravitational potential of a wave function without allocating any device
+ * memory.  No counterpart in the reference: it exists for callers that cannot
+ * call cudaMalloc/cudaFree -- a process whose device memory is owned by
+ * another allocator (a framework's caching pool), or a time-critical loop that
+ * cannot afford cudaMalloc/cudaFree, which may synchronise the device.
+ *   psi: device pointer, res^3 complex128 (interleaved re, im), as for
+ *        ifdm_set_psi; phi: device pointer, res^3 doubles, receives the same
+ *        potential ifdm_get_phi returns for that psi.  mfdm [eV] and xmax
+ *        [Mpc/h, half box] as on the command line.  Runs on `stream`.
+ * Scratch lives in one static device array of IFDM_STATIC_SCRATCH_BYTES that
+ * every GPU loading the library holds until exit, so res is limited to
+ * IFDM_STATIC_MAX_RES (16, 32, 48, 64); larger sizes return
+ * IFDM_ERR_UNSUPPORTED.  All calls share that array: calls that overlap on
+ * the GPU (other streams, other host threads) race and must be serialised by
+ * the caller.  The first call on a device looks up the array's address
+ * (cudaGetSymbolAddress); make it before any stream capture. */
+#define IFDM_STATIC_SCRATCH_BYTES (3u << 20)
+#define IFDM_STATIC_MAX_RES 64
+int ifdm_poisson_static(const double *psi, double *phi, int res, double mfdm, double xmax, void *stream);
+
 #ifdef __cplusplus
 }
 #endif

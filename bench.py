@@ -265,6 +265,35 @@ def run_ours(args):
     passing = ["fp64"] + [p for p in ("mixed", "fp32") if prec_report and prec_report[p]["density_relL2"] <= gate]
     head = min(passing, key=lambda p: res[p]["ms"])
 
+    # adjoint / forward time: record K_a steps (checkpoint every 20), then the
+    # backward sweep (segment replays + adjoint steps), same path as the headline
+    adj = None
+    if args.adjoint_steps > 0:
+        ka = args.adjoint_steps
+        sim = ifdm.Simulation(MFDM, 0.0, XMAX, N, precision=head, device=local)
+        sim.set_psi(psi0, A0)
+        sim.synchronize()
+        t0 = time.perf_counter()
+        sim.record_steps(ka, C, 20)
+        sim.synchronize()
+        t_fwd = time.perf_counter() - t0
+        # any cotangent (the cost does not depend on it), resident on the device like the state
+        gfin = torch.from_numpy(psi0).to(f"cuda:{local}")
+        g0 = torch.empty_like(gfin)
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        sim.adjoint(gfin, g0)
+        sim.synchronize()
+        t_bwd = time.perf_counter() - t0
+        sim.close()
+        del gfin, g0
+        # neither leg copies to or from the host: forward = the recorded steps
+        # (checkpoint copies and step log included), backward = segment replays + adjoint steps
+        adj = {"path": head, "steps": ka, "checkpoint_every": 20, "forward_s": t_fwd, "backward_s": t_bwd,
+               "adjoint_over_forward": t_bwd / t_fwd}
+
+    batch = run_batch(args, head, local) if args.batch_steps > 0 else None
+
     # end to end through the C ABI with host buffers (pinned)
     pin_in = torch.from_numpy(psi0.view(np.float64)).pin_memory()
     pin_out = torch.empty_like(pin_in).pin_memory()
@@ -322,6 +351,8 @@ def run_ours(args):
         "paths": {p: {"value": vals[p], "ms_per_step": res[p]["ms"] / K, "over_fp64": vals[p] / fp64_value,
                       "roofline": roofline(res[p]), "clocks": res[p]["clocks"]} for p in res},
         "precision": prec_report,
+        "adjoint": adj,
+        "batch": batch,
         "roofline": roofline(res[head]),
         "e2e": {"value": e2e_value, "unit": "cell-steps/s", "h2d_bytes_per_step": 16 * cells / K,
                 "d2h_bytes_per_step": 16 * cells / K,
@@ -335,6 +366,64 @@ def run_ours(args):
         dist.destroy_process_group()
     if rank == 0:
         print(json.dumps(out))
+
+
+def run_batch(args, prec, device):
+    """96 realisations of uneven sizes (32 at 32^3, 32 at 48^3, 24 at 64^3, 8 at
+    96^3), each with its own seed and mfdm ~ U[1e-24, 5e-24] eV, g = 0, K steps
+    with per-box step scales that reach a = 0.5 at step 500: one tuned graph
+    launch per K steps against the same runs one at a time (each run's K
+    steps, then a synchronize)."""
+    import numpy as np
+
+    import ifdm_code_b200 as ifdm
+    from ifdm_code_b200.synthetic_ic import zeldovich_psi
+
+    K = args.batch_steps
+    sizes = [32] * 32 + [48] * 32 + [64] * 24 + [96] * 8
+    rng = np.random.default_rng(4000)
+    masses = rng.uniform(1e-24, 5e-24, len(sizes))
+    dts = [dt_scale_for(n, 500, mfdm=float(m)) for n, m in zip(sizes, masses)]
+    psis = [zeldovich_psi(n, xmax=XMAX, seed=4000 + i, a=A0, mfdm=float(m))
+            for i, (n, m) in enumerate(zip(sizes, masses))]
+    sims = [ifdm.Simulation(float(m), 0.0, XMAX, n, precision=prec, device=device) for n, m in zip(sizes, masses)]
+
+    def reset():
+        for sim, psi in zip(sims, psis):
+            sim.set_psi(psi, A0)
+        for sim in sims:
+            sim.synchronize()
+
+    reset()
+    b = ifdm.Batch(sims)
+    tuning = b.tune(5, dts)
+    b.step(K, dts)  # captures and instantiates the graph for K steps
+    b.synchronize()
+    reset()
+    t0 = time.perf_counter()
+    b.step(K, dts)
+    b.synchronize()
+    t_batch = time.perf_counter() - t0
+    out_batch = [sim.get_psi() for sim in sims]
+    info = b.info()
+    b.close()
+    reset()
+    t0 = time.perf_counter()
+    for sim, dt in zip(sims, dts):
+        sim.step(K, dt)
+        sim.synchronize()
+    t_single = time.perf_counter() - t0
+    diff = max(float(np.linalg.norm(sim.get_psi() - o) / np.linalg.norm(o)) for sim, o in zip(sims, out_batch))
+    a_end = min(sim.state()["a"] for sim in sims)
+    for sim in sims:
+        sim.close()
+    cells = float(sum(n ** 3 for n in sizes))
+    return {"path": prec, "boxes": len(sizes), "sizes": {"32": 32, "48": 32, "64": 24, "96": 8}, "steps": K,
+            "value": cells * K / t_batch, "unit": "cell-steps/s", "batch_s": t_batch, "one_at_a_time_s": t_single,
+            "speedup": t_single / t_batch, "one_at_a_time_value": cells * K / t_single,
+            "max_rel_l2_vs_one_at_a_time": diff, "min_a_end": a_end, "tuning": tuning,
+            "items_per_step": info["items_per_step"], "persistent_ctas": info["grid"],
+            "note": "wall clock around one graph replay (state reset between runs, graph captured beforehand)"}
 
 
 def run_reference(args):
@@ -414,6 +503,8 @@ def main():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--profile", action="store_true", help="plain W+K steps of --precision (for ncu)")
     ap.add_argument("--precision", choices=["fp32", "fp64", "mixed"], default="mixed")
+    ap.add_argument("--adjoint-steps", type=int, default=40, help="steps of the adjoint timing (0 skips it)")
+    ap.add_argument("--batch-steps", type=int, default=500, help="steps of the 96-box batch timing (0 skips it)")
     ap.add_argument("--precision-steps", type=int, default=1000,
                     help="steps of the precision gate (density error vs FP64); 0 skips it")
     ap.add_argument("--ref-max-steps", type=int, default=3,

@@ -6,6 +6,6 @@ The compute lives in ``libifdm_b200.so`` (hand-written CUDA, C ABI in
 """
 
 from ._lib import EXPORTS, IfdmError, LIB_PATH, BIN_PATH, load_library  # noqa: F401
-from .simulation import Simulation, fft3d_, supported_res  # noqa: F401
+from .simulation import Batch, Simulation, fft3d_, supported_res  # noqa: F401
 
-__all__ = ["Simulation", "fft3d_", "supported_res", "IfdmError", "load_library", "LIB_PATH", "BIN_PATH"]
+__all__ = ["Simulation", "Batch", "fft3d_", "supported_res", "IfdmError", "load_library", "LIB_PATH", "BIN_PATH"]

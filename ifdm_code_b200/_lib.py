@@ -27,7 +27,10 @@ EXPORTS = [
     "ifdm_params_default", "ifdm_params_from_argv", "ifdm_create", "ifdm_destroy", "ifdm_last_error",
     "ifdm_supported_res", "ifdm_load_ic", "ifdm_load_snapshot", "ifdm_set_psi", "ifdm_get_psi", "ifdm_get_phi",
     "ifdm_get_state", "ifdm_run", "ifdm_step", "ifdm_write_snapshot", "ifdm_synchronize", "ifdm_stream",
-    "ifdm_profile_passes", "ifdm_pass_bytes", "ifdm_fft3d", "ifdm_poisson_static",
+    "ifdm_profile_passes", "ifdm_pass_bytes", "ifdm_fft3d", "ifdm_poisson_static", "ifdm_record_steps",
+    "ifdm_adjoint", "ifdm_batch_create", "ifdm_batch_step", "ifdm_batch_tune", "ifdm_batch_get_tuning",
+    "ifdm_batch_set_tuning", "ifdm_batch_synchronize", "ifdm_batch_info", "ifdm_batch_last_error",
+    "ifdm_batch_destroy",
 ]
 
 
@@ -51,6 +54,13 @@ class State(C.Structure):
         ("a", C.c_double), ("dt_KE", C.c_double), ("dt_PE", C.c_double), ("dt_QI", C.c_double),
         ("max_phi", C.c_double), ("max_rho", C.c_double), ("rhoc", C.c_double), ("steps", C.c_longlong),
         ("criterion", C.c_int), ("device_error", C.c_int),
+    ]
+
+
+class BatchTuning(C.Structure):
+    _fields_ = [
+        ("mode", C.c_int), ("blocks_per_sm", C.c_int), ("group", C.c_int), ("plan", C.c_int * 6),
+        ("ms_per_step", C.c_double),
     ]
 
 
@@ -92,6 +102,19 @@ def load_library() -> C.CDLL:
     lib.ifdm_pass_bytes.argtypes = [P, D, C.c_int]
     lib.ifdm_fft3d.argtypes = [C.c_void_p, C.c_int, C.c_int, C.c_int, C.c_void_p]
     lib.ifdm_poisson_static.argtypes = [C.c_void_p, C.c_void_p, C.c_int, C.c_double, C.c_double, C.c_void_p]
+    lib.ifdm_record_steps.argtypes = [P, C.c_int, C.c_double, C.c_int]
+    lib.ifdm_adjoint.argtypes = [P, C.c_void_p, C.c_void_p]
+    lib.ifdm_batch_create.argtypes = [C.POINTER(P), C.c_int, C.POINTER(P)]
+    lib.ifdm_batch_step.argtypes = [P, C.c_int, D]
+    lib.ifdm_batch_tune.argtypes = [P, C.c_int, D, C.POINTER(BatchTuning)]
+    lib.ifdm_batch_get_tuning.argtypes = [P, C.POINTER(BatchTuning)]
+    lib.ifdm_batch_set_tuning.argtypes = [P, C.POINTER(BatchTuning)]
+    lib.ifdm_batch_synchronize.argtypes = [P]
+    lib.ifdm_batch_info.argtypes = [P, C.POINTER(C.c_longlong), C.POINTER(C.c_int)]
+    lib.ifdm_batch_last_error.argtypes = [P]
+    lib.ifdm_batch_last_error.restype = C.c_char_p
+    lib.ifdm_batch_destroy.argtypes = [P]
+    lib.ifdm_batch_destroy.restype = None
     for name in EXPORTS:
         getattr(lib, name)  # raises AttributeError if an export is missing
     _lib = lib

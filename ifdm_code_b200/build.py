@@ -30,7 +30,8 @@ NVCC_FLAGS = ARCH + ["-O3", "-lineinfo", "-std=c++17", "-Xcompiler", "-fPIC", "-
 PER_FILE = {"ic_pipeline.cu": ["--fmad=false"]}
 CXX_FLAGS = ["-O2", "-fPIC", "-std=c++17", "-Wall", "-I" + CSRC, "-I" + INC]
 
-CU_SOURCES = ["step_engine.cu", "ic_pipeline.cu", "static_poisson.cu"]
+CU_SOURCES = ["step_engine.cu", "batch_engine.cu", "batch_fp64.cu", "batch_fp32.cu", "batch_mixed.cu",
+              "ic_pipeline.cu", "static_poisson.cu"]
 CPP_SOURCES = ["ifdm_api.cpp", "io.cpp"]
 
 

@@ -10,7 +10,8 @@
 // Thread (l = tid % L, t = tid / L) owns E = N / T elements of line l; a
 // radix-R stage runs E / R butterflies per thread (Stockham autosort, so no
 // bit reversal pass).  Twiddles come from a per-size table of
-// exp(-2 pi i m / N) built on the host in long double and rounded once.
+// exp(-2 pi i m / N) built on the host in long double and rounded once (FP32
+// tables also carry the rounding remainders, see twmul).
 #pragma once
 
 #include <cuda_runtime.h>
@@ -58,6 +59,14 @@ template <> struct Plan<128> { static constexpr int E = 8, NST = 3; static const
 template <> struct Plan<256> { static constexpr int E = 8, NST = 3; static constexpr int R[3] = {8, 4, 8}; };
 template <> struct Plan<512> { static constexpr int E = 8, NST = 3; static constexpr int R[3] = {8, 8, 8}; };
 
+// Alternative radix orders with the same elements per thread (V = 1), for the
+// batch autotuner; V = 0 and sizes without an alternative are Plan<N>.
+template <int N, int V> struct PlanV : Plan<N> {};
+template <> struct PlanV<32, 1> { static constexpr int E = 8, NST = 2; static constexpr int R[2] = {4, 8}; };
+template <> struct PlanV<48, 1> { static constexpr int E = 12, NST = 3; static constexpr int R[3] = {3, 4, 4}; };
+template <> struct PlanV<64, 1> { static constexpr int E = 8, NST = 3; static constexpr int R[3] = {4, 4, 4}; };
+template <> struct PlanV<96, 1> { static constexpr int E = 12, NST = 4; static constexpr int R[4] = {3, 4, 2, 4}; };
+
 // ------------------------------------------------------------- butterflies --
 template <int RAD, int DIR> struct Bfly;
 
@@ -80,14 +89,27 @@ template <int DIR> struct Bfly<4, DIR> {
     }
 };
 
+// x * c for a real constant c = hi + lo.  FP32 adds the product with the
+// rounding remainder lo of the constant: a constant rounded to FP32 would
+// scale every butterfly output the same way at every step (a systematic bias
+// of ~1e-8 per stage, e.g. a steady loss of norm), while the remaining product
+// roundings vary with the data.  In FP64 lo is 0 and this is x * hi.
+__device__ __forceinline__ double mulk(double x, double hi, double) { return x * hi; }
+__device__ __forceinline__ float mulk(float x, float hi, float lo) { return fmaf(x, hi, x * lo); }
+template <typename R> struct KSplit {
+    R hi, lo;
+    __host__ __device__ constexpr KSplit(double c) : hi(R(c)), lo(R(c - double(R(c)))) {}
+};
+
 template <int DIR> struct Bfly<3, DIR> {
     template <typename C> __device__ __forceinline__ static void run(C *v) {
         using R = decltype(v[0].x);
         const R h = R(0.5);
-        const R s3 = R(0.86602540378443864676372317075294);  // sqrt(3)/2
+        constexpr KSplit<R> s3(0.86602540378443864676372317075294);  // sqrt(3)/2
         C t1 = v[1] + v[2];
         C t2 = v[0] - cscale(t1, h);
-        C t3 = cscale(mul_i<DIR>(v[1] - v[2]), s3);
+        const C d = mul_i<DIR>(v[1] - v[2]);
+        C t3 = mkc(mulk(d.x, s3.hi, s3.lo), mulk(d.y, s3.hi, s3.lo));
         v[0] = v[0] + t1;
         v[1] = t2 + t3;
         v[2] = t2 - t3;
@@ -97,7 +119,7 @@ template <int DIR> struct Bfly<3, DIR> {
 template <int DIR> struct Bfly<8, DIR> {
     template <typename C> __device__ __forceinline__ static void run(C *v) {
         using R = decltype(v[0].x);
-        const R q = R(0.70710678118654752440084436210485);  // 1/sqrt(2)
+        constexpr KSplit<R> q(0.70710678118654752440084436210485);  // 1/sqrt(2)
         C a0 = v[0] + v[4], a1 = v[0] - v[4];
         C a2 = v[2] + v[6], a3 = mul_i<DIR>(v[2] - v[6]);
         C a4 = v[1] + v[5], a5 = v[1] - v[5];
@@ -107,11 +129,11 @@ template <int DIR> struct Bfly<8, DIR> {
         // c1 *= w8, c2 *= w8^2 = -/+i, c3 *= w8^3 ; w8 = (1 -/+ i)/sqrt2
         C w1, w3;
         if (DIR < 0) {
-            w1 = mkc((c1.x + c1.y) * q, (c1.y - c1.x) * q);
-            w3 = mkc((c3.y - c3.x) * q, -(c3.x + c3.y) * q);
+            w1 = mkc(mulk(c1.x + c1.y, q.hi, q.lo), mulk(c1.y - c1.x, q.hi, q.lo));
+            w3 = mkc(mulk(c3.y - c3.x, q.hi, q.lo), -mulk(c3.x + c3.y, q.hi, q.lo));
         } else {
-            w1 = mkc((c1.x - c1.y) * q, (c1.x + c1.y) * q);
-            w3 = mkc(-(c3.x + c3.y) * q, (c3.x - c3.y) * q);
+            w1 = mkc(mulk(c1.x - c1.y, q.hi, q.lo), mulk(c1.x + c1.y, q.hi, q.lo));
+            w3 = mkc(-mulk(c3.x + c3.y, q.hi, q.lo), mulk(c3.x - c3.y, q.hi, q.lo));
         }
         C w2 = mul_i<DIR>(c2);
         v[0] = b0 + c0;
@@ -131,6 +153,23 @@ template <int DIR, typename C> __device__ __forceinline__ C twiddle(const C *__r
     return DIR < 0 ? w : cconj(w);
 }
 
+// a * exp(DIR * 2 pi i m / TN).  FP64 tables hold one double2 per m.  FP32
+// tables hold two float2 per m, the rounded twiddle and its rounding
+// remainder (one 16-byte load), and the remainder is folded into the product,
+// so the transform is the exact DFT up to the product's own rounding (a
+// twiddle table rounded to FP32 alone is a fixed operator error that every
+// step repeats).
+template <int DIR, int TN> __device__ __forceinline__ double2 twmul(double2 a, const double2 *__restrict__ tw, int m) {
+    return cmul(a, twiddle<DIR>(tw, m));
+}
+template <int DIR, int TN> __device__ __forceinline__ float2 twmul(float2 a, const float2 *__restrict__ tw, int m) {
+    const float4 q = __ldg(reinterpret_cast<const float4 *>(tw) + m);
+    const float2 h = make_float2(q.x, q.y), r = make_float2(q.z, q.w);
+    const float hy = DIR < 0 ? h.y : -h.y, ry = DIR < 0 ? r.y : -r.y;
+    const float cr = fmaf(a.x, r.x, -a.y * ry), ci = fmaf(a.x, ry, a.y * r.x);
+    return make_float2(fmaf(a.x, h.x, fmaf(-a.y, hy, cr)), fmaf(a.x, hy, fmaf(a.y, h.x, ci)));
+}
+
 // One Stockham stage: radix RAD, NS = product of the previous radices.
 template <typename C, int N, int E, int DIR, int L, int LP, int RAD, int NS>
 __device__ __forceinline__ void stockham_stage(C *sm, const C *__restrict__ tw, int l, int t, bool active) {
@@ -147,7 +186,7 @@ __device__ __forceinline__ void stockham_stage(C *sm, const C *__restrict__ tw, 
 #pragma unroll
             for (int r = 0; r < RAD; ++r) {
                 C a = sm[(j + r * STRIDE) * LP + l];
-                if (NS > 1 && r > 0) a = cmul(a, twiddle<DIR>(tw, k * r * TWSTEP));
+                if (NS > 1 && r > 0) a = twmul<DIR, N>(a, tw, k * r * TWSTEP);
                 v[b * RAD + r] = a;
             }
             Bfly<RAD, DIR>::run(&v[b * RAD]);
@@ -167,14 +206,14 @@ __device__ __forceinline__ void stockham_stage(C *sm, const C *__restrict__ tw, 
     __syncthreads();
 }
 
-template <typename C, int N, int E, int DIR, int L, int LP, int S, int NS>
+template <typename C, int N, int E, int DIR, int L, int LP, int S, int NS, class P = Plan<N>>
 struct StageLoop {
     __device__ __forceinline__ static void run(C *sm, const C *__restrict__ tw, int l, int t, bool active) {
-        if constexpr (S < Plan<N>::NST) {
-            constexpr int RAD = Plan<N>::R[S];
+        if constexpr (S < P::NST) {
+            constexpr int RAD = P::R[S];
             static_assert(E % RAD == 0, "elements per thread must be a multiple of every radix");
             stockham_stage<C, N, E, DIR, L, LP, RAD, NS>(sm, tw, l, t, active);
-            StageLoop<C, N, E, DIR, L, LP, S + 1, NS * RAD>::run(sm, tw, l, t, active);
+            StageLoop<C, N, E, DIR, L, LP, S + 1, NS * RAD, P>::run(sm, tw, l, t, active);
         }
     }
 };
@@ -193,13 +232,13 @@ template <int N, int T> __host__ __device__ constexpr int elems_for(int) {
 // Transform all L lines of the tile in place, E elements per thread (threads
 // tid < L * (N / E) work; the rest only join the barriers).  Caller must
 // __syncthreads() before (tile written); the tile is synced on return.
-template <typename C, int N, int E, int DIR, int L, int LP>
+template <typename C, int N, int E, int DIR, int L, int LP, class P = Plan<N>>
 __device__ __forceinline__ void fft_tile(C *sm, const C *__restrict__ tw) {
     constexpr int T = N / E;
     const int tid = threadIdx.x;
     const int l = tid % L;
     const int t = tid / L;
-    StageLoop<C, N, E, DIR, L, LP, 0, 1>::run(sm, tw, l, t, t < T);
+    StageLoop<C, N, E, DIR, L, LP, 0, 1, P>::run(sm, tw, l, t, t < T);
 }
 
 // ------------------------------------------------ register-resident chain --
@@ -226,7 +265,7 @@ __device__ __forceinline__ void stage_compute(C *v, const C *__restrict__ tw, in
         const int k = (t + T * b) % NS;
         if (NS > 1) {
 #pragma unroll
-            for (int r = 1; r < RAD; ++r) v[b * RAD + r] = cmul(v[b * RAD + r], twiddle<DIR>(tw, k * r * TWSTEP));
+            for (int r = 1; r < RAD; ++r) v[b * RAD + r] = twmul<DIR, N>(v[b * RAD + r], tw, k * r * TWSTEP);
         }
         Bfly<RAD, DIR>::run(&v[b * RAD]);
     }

@@ -11,6 +11,7 @@
 #include <string>
 #include <vector>
 
+#include "batch_engine.hpp"
 #include "ic_pipeline.hpp"
 #include "io.hpp"
 #include "physics.hpp"
@@ -163,7 +164,20 @@ int ifdm_set_psi(ifdm_ctx *c, const double *psi, double a, double rhoc) {
 }
 
 // psi of the current state into a host buffer; which: 1 snapshot kick, 2 pending kick
+static bool is_device_ptr(const void *p) {
+    cudaPointerAttributes attr{};
+    const bool dev = cudaPointerGetAttributes(&attr, p) == cudaSuccess && attr.type == cudaMemoryTypeDevice;
+    cudaGetLastError();
+    return dev;
+}
+
+// psi of the current state into a host or device buffer; which: 1 snapshot kick, 2 pending kick
 static int psi_to_host(ifdm_ctx *c, double *host, int which) {
+    if (is_device_ptr(host)) {
+        CTX_STR(c, IFDM_ERR_CUDA, c->eng.psi_out(host, which));
+        CTX_CUDA(c, cudaStreamSynchronize(c->stream));
+        return IFDM_OK;
+    }
     if (ensure_out(c)) return IFDM_ERR_CUDA;
     CTX_STR(c, IFDM_ERR_CUDA, c->eng.psi_out(c->d_out, which));
     CTX_CUDA(c, cudaMemcpyAsync(host, c->d_out, c->eng.n3() * 2 * sizeof(double), cudaMemcpyDeviceToHost, c->stream));
@@ -407,6 +421,160 @@ int ifdm_pass_bytes(ifdm_ctx *c, double *bytes_out, int cap) {
     auto b = c->eng.pass_bytes();
     for (int i = 0; i < (int)b.size() && i < cap; ++i) bytes_out[i] = b[i];
     return (int)b.size();
+}
+
+int ifdm_record_steps(ifdm_ctx *c, int nsteps, double dt_scale, int checkpoint_every) {
+    if (!c || nsteps <= 0 || checkpoint_every <= 0) return IFDM_ERR_ARGS;
+    if (!c->have_psi) return fail(c, IFDM_ERR_STATE, "no wave function loaded");
+    CTX_STR(c, IFDM_ERR_CUDA, c->eng.record(nsteps, dt_scale, checkpoint_every));
+    return IFDM_OK;
+}
+
+int ifdm_adjoint(ifdm_ctx *c, const double *g_final, double *g0) {
+    if (!c || !g_final || !g0) return IFDM_ERR_ARGS;
+    if (c->eng.recorded_steps() <= 0) return fail(c, IFDM_ERR_STATE, "ifdm_adjoint: no recorded steps");
+    const size_t bytes = c->eng.n3() * 2 * sizeof(double);
+    const bool din = is_device_ptr(g_final), dout = is_device_ptr(g0);
+    double *tin = nullptr, *tout = nullptr;
+    if (!din) {
+        CTX_CUDA(c, cudaMalloc(&tin, bytes));
+        CTX_CUDA(c, cudaMemcpyAsync(tin, g_final, bytes, cudaMemcpyHostToDevice, c->stream));
+    }
+    if (!dout) {
+        if (cudaMalloc(&tout, bytes) != cudaSuccess) {
+            cudaFree(tin);
+            return fail(c, IFDM_ERR_CUDA, "ifdm_adjoint: device buffer allocation failed");
+        }
+    }
+    std::string e = c->eng.adjoint(din ? g_final : tin, dout ? g0 : tout);
+    if (e.empty() && !dout) {
+        cudaError_t ce = cudaMemcpyAsync(g0, tout, bytes, cudaMemcpyDeviceToHost, c->stream);
+        if (ce != cudaSuccess) e = std::string("cudaMemcpyAsync: ") + cudaGetErrorString(ce);
+    }
+    cudaError_t ce = cudaStreamSynchronize(c->stream);
+    if (e.empty() && ce != cudaSuccess) e = std::string("cudaStreamSynchronize: ") + cudaGetErrorString(ce);
+    cudaFree(tin);
+    cudaFree(tout);
+    if (!e.empty()) return fail(c, IFDM_ERR_CUDA, e);
+    TState t{};
+    CTX_STR(c, IFDM_ERR_CUDA, c->eng.read_state(t));
+    if (t.err) return fail(c, IFDM_ERR_DEVICE, "a device-side check failed during the adjoint");
+    return IFDM_OK;
+}
+
+// ------------------------------------------------------------------ batches --
+struct ifdm_batch {
+    std::vector<ifdm_ctx *> ctx;
+    cudaStream_t stream = nullptr;
+    BatchEngine eng;
+    std::string err;
+};
+
+static int bfail(ifdm_batch *b, int code, const std::string &msg) {
+    if (b) b->err = msg;
+    return code;
+}
+
+int ifdm_batch_create(ifdm_ctx *const *ctxs, int n, ifdm_batch **out) {
+    if (!out) return IFDM_ERR_ARGS;
+    *out = nullptr;
+    if (!ctxs || n <= 0) return IFDM_ERR_ARGS;
+    for (int i = 0; i < n; ++i)
+        if (!ctxs[i]) return IFDM_ERR_ARGS;
+    auto b = std::make_unique<ifdm_batch>();
+    std::vector<StepEngine *> engines;
+    for (int i = 0; i < n; ++i) {
+        b->ctx.push_back(ctxs[i]);
+        engines.push_back(&ctxs[i]->eng);
+    }
+    ifdm_batch *raw = b.release();
+    *out = raw;
+    for (int i = 0; i < n; ++i)
+        if (ctxs[i]->p.device != ctxs[0]->p.device) return bfail(raw, IFDM_ERR_ARGS, "batch: contexts on different devices");
+    if (cudaSetDevice(ctxs[0]->p.device) != cudaSuccess ||
+        cudaStreamCreateWithFlags(&raw->stream, cudaStreamNonBlocking) != cudaSuccess)
+        return bfail(raw, IFDM_ERR_CUDA, "batch: stream creation failed");
+    std::string e = raw->eng.init(engines, raw->stream);
+    if (!e.empty()) {
+        const bool shape = e.find("batch size") != std::string::npos || e.find("precision") != std::string::npos;
+        return bfail(raw, shape ? IFDM_ERR_UNSUPPORTED : IFDM_ERR_CUDA, e);
+    }
+    return IFDM_OK;
+}
+
+int ifdm_batch_step(ifdm_batch *b, int nsteps, const double *dt_scale) {
+    if (!b || nsteps < 0 || !dt_scale) return IFDM_ERR_ARGS;
+    for (auto *c : b->ctx)
+        if (!c->have_psi) return bfail(b, IFDM_ERR_STATE, "batch: a context has no wave function");
+    if (cudaSetDevice(b->ctx[0]->p.device) != cudaSuccess) return bfail(b, IFDM_ERR_CUDA, "cudaSetDevice failed");
+    std::string e = b->eng.step(nsteps, dt_scale);
+    return e.empty() ? IFDM_OK : bfail(b, IFDM_ERR_CUDA, e);
+}
+
+static void knobs_to_tuning(const BatchKnobs &k, ifdm_batch_tuning *t) {
+    t->mode = k.mode;
+    t->blocks_per_sm = k.blocks_per_sm;
+    t->group = k.group;
+    for (int i = 0; i < kBatchSizes; ++i) t->plan[i] = k.plan[i];
+}
+
+int ifdm_batch_tune(ifdm_batch *b, int trial_steps, const double *dt_scale, ifdm_batch_tuning *out) {
+    if (!b || trial_steps <= 0 || !dt_scale) return IFDM_ERR_ARGS;
+    for (auto *c : b->ctx)
+        if (!c->have_psi) return bfail(b, IFDM_ERR_STATE, "batch: a context has no wave function");
+    double ms = 0;
+    std::string e = b->eng.tune(trial_steps, dt_scale, &ms);
+    if (!e.empty()) return bfail(b, e.find("gave up") != std::string::npos ? IFDM_ERR_DEVICE : IFDM_ERR_CUDA, e);
+    if (out) {
+        knobs_to_tuning(b->eng.knobs, out);
+        out->ms_per_step = ms;
+    }
+    return IFDM_OK;
+}
+
+int ifdm_batch_get_tuning(ifdm_batch *b, ifdm_batch_tuning *out) {
+    if (!b || !out) return IFDM_ERR_ARGS;
+    knobs_to_tuning(b->eng.knobs, out);
+    out->ms_per_step = 0;
+    return IFDM_OK;
+}
+
+int ifdm_batch_set_tuning(ifdm_batch *b, const ifdm_batch_tuning *t) {
+    if (!b || !t || t->blocks_per_sm < 1 || t->group < 0 || (t->mode != 0 && t->mode != 1)) return IFDM_ERR_ARGS;
+    for (int i = 0; i < kBatchSizes; ++i)
+        if (t->plan[i] != 0 && t->plan[i] != 1) return IFDM_ERR_ARGS;
+    b->eng.knobs.mode = t->mode;
+    b->eng.knobs.blocks_per_sm = t->blocks_per_sm;
+    b->eng.knobs.group = t->group;
+    for (int i = 0; i < kBatchSizes; ++i) b->eng.knobs.plan[i] = t->plan[i];
+    return IFDM_OK;
+}
+
+int ifdm_batch_synchronize(ifdm_batch *b) {
+    if (!b) return IFDM_ERR_ARGS;
+    int st = 0;
+    std::string e = b->eng.check_status(&st);
+    if (!e.empty()) return bfail(b, IFDM_ERR_CUDA, e);
+    if (st) return bfail(b, IFDM_ERR_DEVICE, "batch: a dependency wait of the batch kernel gave up");
+    return IFDM_OK;
+}
+
+int ifdm_batch_info(ifdm_batch *b, long long *items_per_step, int *grid) {
+    if (!b) return IFDM_ERR_ARGS;
+    if (items_per_step) *items_per_step = b->eng.items_per_step();
+    if (grid) *grid = b->eng.grid();
+    return IFDM_OK;
+}
+
+const char *ifdm_batch_last_error(const ifdm_batch *b) { return b ? b->err.c_str() : "null batch"; }
+
+void ifdm_batch_destroy(ifdm_batch *b) {
+    if (!b) return;
+    if (b->stream) {
+        cudaStreamSynchronize(b->stream);
+        cudaStreamDestroy(b->stream);
+    }
+    delete b;  // the engine's graphs and buffers do not refer to the stream
 }
 
 int ifdm_fft3d(void *data, int n, int precision, int sign, void *stream) {

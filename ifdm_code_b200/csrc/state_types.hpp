@@ -15,6 +15,8 @@ struct TState {
     double cre, cim;            // offset c removed before the forward FFT, added after the inverse
     double cnext_re, cnext_im;  // mean of the kicked field, from the k = 0 coefficient (next step's c)
     double mu;                  // mean |psi_s|^2 (conserved), subtracted from the Poisson source
+    double alpha;               // dither phase added to this step's kick (FP32 mode, else 0)
+    double gphase, gphase_prev; // accumulated dither after / before this step's kick (mod 2 pi)
     double maxphi, maxrho;      // natural units, inputs of the latest timestep
     unsigned long long maxphi_bits, maxrho_bits; // atomicMax targets (scaled, non-negative doubles)
     long long steps;
@@ -35,6 +37,7 @@ struct Phys {
     double Phi0, S2;  // natural units of phi_s and |psi_s|^2
     double dt_scale;  // fixed-step mode multiplier (1 = reference)
     int N;
+    int dither;       // 1: rotate psi by a pseudo-random global phase every step (FP32 mode)
     int limit;        // quadrature interval limit on the device
 };
 

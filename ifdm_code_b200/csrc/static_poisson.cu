@@ -59,6 +59,8 @@ template <int N> static size_t static_bytes_needed() {
 template <int N>
 static int static_poisson_n(unsigned char *base, const double2 *psi, double *phi, double phi0, cudaStream_t s) {
     using TL = Tile<double, double, N>;
+    static_assert(TileZ<double, double, N>::L == TL::L && TileZ<double, double, N>::NT == TL::NT,
+                  "FP64 row tiles equal the line tiles");
     constexpr int NH = N / 2 + 1;
     constexpr int NHP = half_pitch<double>(N);
     static_assert(kOffPart + 3 * sizeof(double) * (size_t(N) * N / TL::L) <= kOffTw, "partial sums must fit");

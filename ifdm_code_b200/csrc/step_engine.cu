@@ -4,6 +4,8 @@
 #include "step_engine.hpp"
 #include "timestep.cuh"
 #include "tma_passes.cuh"
+#include "zpass_pipe.cuh"
+#include "adjoint_kernels.cuh"
 
 #include <cudaTypedefs.h>
 
@@ -12,6 +14,7 @@
 #include <cstdlib>
 #include <cstring>
 #include <type_traits>
+#include <algorithm>
 
 namespace ifdm {
 
@@ -36,19 +39,21 @@ bool supported_n(int n) {
 template <typename R_, typename K_, int N> struct Box {
     using R = R_;
     using K = K_;
-    using TL = Tile<R, K, N>;
+    using TL = Tile<R, K, N>;   // y/x passes (strided lines)
+    using TZ = TileZ<R, K, N>;  // z passes (contiguous rows)
     using C = cx<K>;
     using G = cx<R>;
     static constexpr int NH = N / 2 + 1;
     static constexpr int NHP = half_pitch<R>(N);
     static constexpr size_t SM = TL::SMEM;
-    static constexpr size_t SM9 = TL::SMEM9;
+    static constexpr size_t SMZ = TZ::SMEM;
+    static constexpr size_t SMZ9 = TZ::SMEM9;
     // every launch covers its array exactly: no partial tiles
-    static_assert((N * N) % TL::L == 0, "z/y/x tiles must divide N^2 lines");
+    static_assert((N * N) % TL::L == 0 && (N * N) % TZ::L == 0, "z/y/x tiles must divide N^2 lines");
     static_assert((N * NHP) % TL::L == 0, "half-spectrum tiles must divide N*NHP lines");
     static_assert(NHP >= NH, "half-spectrum pitch");
-    static_assert(TL::NT <= 1024, "block size");
-    static_assert(SM9 <= 227 * 1024, "shared memory per block");
+    static_assert(TL::NT <= 1024 && TZ::NT <= 1024, "block size");
+    static_assert(SM <= 227 * 1024 && SMZ9 <= 227 * 1024, "shared memory per block");
 
     template <typename Kern> static cudaError_t prep(Kern kern, size_t smem) {
         return cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
@@ -57,83 +62,142 @@ template <typename R_, typename K_, int N> struct Box {
     static std::string configure() {
         static bool done = false;
         if (done) return "";
-        CUDA_TRY(prep(k_kick_fft_z<R, K, N>, SM));
+        CUDA_TRY(prep(k_kick_fft_z<R, K, N>, SMZ));
         CUDA_TRY(prep(k_fft_yx<R, K, N, -1, 1>, SM));
         CUDA_TRY(prep(k_fft_yx<R, K, N, +1, 1>, SM));
         CUDA_TRY(prep(k_fft_yx<R, K, N, -1, 2>, SM));
         CUDA_TRY(prep(k_fft_yx<R, K, N, +1, 2>, SM));
         CUDA_TRY(prep(k_fft_x_drift<R, K, N>, SM));
-        CUDA_TRY(prep(k_density_r2c_z<R, K, N, true>, SM));
-        CUDA_TRY(prep(k_density_r2c_z<R, K, N, false>, SM));
+        CUDA_TRY(prep(k_density_r2c_z<R, K, N, true>, SMZ));
+        CUDA_TRY(prep(k_density_r2c_z<R, K, N, false>, SMZ));
         CUDA_TRY(prep(k_fft_x_poisson<R, K, N>, SM));
-        CUDA_TRY(prep(k_c2r_z_phi<R, K, N>, SM9));
-        CUDA_TRY(prep(k_fft_z<R, K, N, -1>, SM));
-        CUDA_TRY(prep(k_fft_z<R, K, N, +1>, SM));
+        CUDA_TRY(prep(k_c2r_z_phi<R, K, N>, SMZ9));
+        CUDA_TRY(prep(k_fft_z<R, K, N, -1>, SMZ));
+        CUDA_TRY(prep(k_fft_z<R, K, N, +1>, SMZ));
+        CUDA_TRY(prep(k_source_r2c_z<R, K, N>, SMZ));
+        int dev = 0, sms = 0;
+        CUDA_TRY(cudaGetDevice(&dev));
+        CUDA_TRY(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));
+        if constexpr (kZPipe) {
+            using ZP = ZPipe<R, N>;
+            CUDA_TRY(prep(k_density_r2c_z_pipe<R, N>, ZP::SMEM5));
+            int b5 = 0;
+            CUDA_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&b5, k_density_r2c_z_pipe<R, N>, ZP::NT, ZP::SMEM5));
+            zgrid = sms * (b5 > 0 ? b5 : 1);
+        }
         if constexpr (kTma) {
             CUDA_TRY(prep(k_yx_tma<R, K, N, 1, 0, -1>, TT::SMEM));
             CUDA_TRY(prep(k_yx_tma<R, K, N, 1, 0, +1>, TT::SMEM));
-            CUDA_TRY(prep(k_yx_tma<R, K, N, 2, 1, 0>, TT::SMEM));
-            CUDA_TRY(prep(k_yx_tma<R, K, N, 2, 2, 0>, TT::SMEM));
+            CUDA_TRY(prep(k_yx_tma<R, K, N, 2, 1, 0>, TX::SMEM));
+            CUDA_TRY(prep(k_yx_tma<R, K, N, 2, 2, 0>, TX::SMEM));
+            // persistent grids: every block resident at once (one wave)
+            int by = 0, bx = 0;
+            CUDA_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&by, k_yx_tma<R, K, N, 1, 0, -1>, TT::NT, TT::SMEM));
+            CUDA_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&bx, k_yx_tma<R, K, N, 2, 1, 0>, TX::NT, TX::SMEM));
+            ygrid = sms * (by > 0 ? by : 1);
+            xgrid = sms * (bx > 0 ? bx : 1);
         }
         done = true;
         return "";
     }
 
-    // TMA-pipelined y/x passes for N >= 128
+    // TMA-pipelined y/x passes for N >= 128.  The cp.async-pipelined P5 is
+    // used in FP32 only: measured at 512^3 it cut FP32 P5 from 1.42 to 1.02 ms
+    // but slowed the FP64 z passes (one 2-slot block per SM hides less latency
+    // than three plain blocks), and pipelined P1/P9 gained nothing.
     static constexpr bool kTma = N >= 128;
-    using TT = TmaTile<R, K, N>;
+    static constexpr bool kZPipe = N >= 128 && std::is_same<R, float>::value && std::is_same<K, float>::value;
+    using TT = TmaTile<R, K, N, 1>;
+    using TX = TmaTile<R, K, N, 2>;
+    static inline int zgrid = 0;             // persistent grid of the pipelined P5
+    static inline int ygrid = 0, xgrid = 0;  // persistent grids of the TMA y and x passes
 
-    static unsigned zblocks() { return unsigned(size_t(N) * N / TL::L); }
+    // lines per TMA tile of the y and x passes (the inner box extent of their maps)
+    static void tma_lines(int &ly, int &lx) {
+        ly = TT::L;
+        lx = TX::L;
+    }
+
+    static unsigned zblocks() { return unsigned(size_t(N) * N / TL::L); }  // y-pass tiles
+    static unsigned zrows() { return unsigned(size_t(N) * N / TZ::L); }    // z-pass tiles
     static unsigned hblocks() { return unsigned(size_t(N) * NHP / TL::L); }
 
     // one pass by index 1..9; tm: TMA maps (psi y, psi x, rho y, rho x) or null
     static void pass(int p, cudaStream_t s, G *psi, R *phi, G *rhok, TState *ts, const C *drift, const C *tw,
-                     const C *twh, long wr, int wt, const CUtensorMap *tm = nullptr, int grid = 0) {
+                     const C *twh, long wr, int wt, const CUtensorMap *tm = nullptr) {
         const unsigned nt = TL::NT;
+        if constexpr (kZPipe) {
+            if (tm && p == 5 && std::getenv("IFDM_NO_ZPIPE") == nullptr) {
+                using ZP = ZPipe<R, N>;
+                const int nz = int(size_t(N) * N / ZP::L);
+                k_density_r2c_z_pipe<R, N><<<zgrid, ZP::NT, ZP::SMEM5, s>>>(psi, rhok, ts, tw, twh, nz);
+                return;
+            }
+        }
         if constexpr (kTma) {
             if (tm && (p == 2 || p == 3 || p == 4 || p == 6 || p == 7 || p == 8)) {
-                const int tc = int(size_t(N) * N / TT::L), th = int(size_t(N) * NHP / TT::L);
-                const unsigned g2 = unsigned(grid), tn = TT::NT;
-                const size_t sm = TT::SMEM;
+                // y tiles (TT) and x tiles (TX) may differ in lines per tile
+                const int tcy = int(size_t(N) * N / TT::L), thy = int(size_t(N) * NHP / TT::L);
+                const int tcx = int(size_t(N) * N / TX::L), thx = int(size_t(N) * NHP / TX::L);
+                const unsigned gy = unsigned(ygrid), gx = unsigned(xgrid), ny = TT::NT, nx = TX::NT;
+                const size_t sy = TT::SMEM, sx = TX::SMEM;
                 switch (p) {
-                    case 2: k_yx_tma<R, K, N, 1, 0, -1><<<g2, tn, sm, s>>>(tm[0], psi, N, N, tc, ts, 2, drift, tw); break;
-                    case 3: k_yx_tma<R, K, N, 2, 1, 0><<<g2, tn, sm, s>>>(tm[1], psi, N, N, tc, ts, 3, drift, tw); break;
-                    case 4: k_yx_tma<R, K, N, 1, 0, +1><<<g2, tn, sm, s>>>(tm[0], psi, N, N, tc, ts, 4, drift, tw); break;
-                    case 6: k_yx_tma<R, K, N, 1, 0, -1><<<g2, tn, sm, s>>>(tm[2], rhok, NHP, NH, th, ts, 6, drift, tw); break;
-                    case 7: k_yx_tma<R, K, N, 2, 2, 0><<<g2, tn, sm, s>>>(tm[3], rhok, NHP, NH, th, ts, 7, drift, tw); break;
-                    case 8: k_yx_tma<R, K, N, 1, 0, +1><<<g2, tn, sm, s>>>(tm[2], rhok, NHP, NH, th, ts, 8, drift, tw); break;
+                    case 2: k_yx_tma<R, K, N, 1, 0, -1><<<gy, ny, sy, s>>>(tm[0], psi, N, N, tcy, ts, 2, drift, tw); break;
+                    case 3: k_yx_tma<R, K, N, 2, 1, 0><<<gx, nx, sx, s>>>(tm[1], psi, N, N, tcx, ts, 3, drift, tw); break;
+                    case 4: k_yx_tma<R, K, N, 1, 0, +1><<<gy, ny, sy, s>>>(tm[0], psi, N, N, tcy, ts, 4, drift, tw); break;
+                    case 6: k_yx_tma<R, K, N, 1, 0, -1><<<gy, ny, sy, s>>>(tm[2], rhok, NHP, NH, thy, ts, 6, drift, tw); break;
+                    case 7: k_yx_tma<R, K, N, 2, 2, 0><<<gx, nx, sx, s>>>(tm[3], rhok, NHP, NH, thx, ts, 7, drift, tw); break;
+                    case 8: k_yx_tma<R, K, N, 1, 0, +1><<<gy, ny, sy, s>>>(tm[2], rhok, NHP, NH, thy, ts, 8, drift, tw); break;
                 }
                 return;
             }
         }
         switch (p) {
-            case 1: k_kick_fft_z<R, K, N><<<zblocks(), nt, SM, s>>>(psi, phi, ts, tw); break;
+            case 1: k_kick_fft_z<R, K, N><<<zrows(), TZ::NT, SMZ, s>>>(psi, phi, ts, tw); break;
             case 2: k_fft_yx<R, K, N, -1, 1><<<zblocks(), nt, SM, s>>>(psi, N, N, ts, 2, tw); break;
             case 3: k_fft_x_drift<R, K, N><<<zblocks(), nt, SM, s>>>(psi, drift, ts, tw); break;
             case 4: k_fft_yx<R, K, N, +1, 1><<<zblocks(), nt, SM, s>>>(psi, N, N, ts, 4, tw); break;
-            case 5: k_density_r2c_z<R, K, N, true><<<zblocks(), nt, SM, s>>>(psi, rhok, ts, nullptr, tw, twh); break;
+            case 5:
+                k_density_r2c_z<R, K, N, true><<<zrows(), TZ::NT, SMZ, s>>>(psi, rhok, ts, nullptr, tw, twh);
+                break;
             case 6: k_fft_yx<R, K, N, -1, 1><<<hblocks(), nt, SM, s>>>(rhok, NHP, NH, ts, 6, tw); break;
             case 7: k_fft_x_poisson<R, K, N><<<hblocks(), nt, SM, s>>>(rhok, ts, tw); break;
             case 8: k_fft_yx<R, K, N, +1, 1><<<hblocks(), nt, SM, s>>>(rhok, NHP, NH, ts, 8, tw); break;
-            case 9: k_c2r_z_phi<R, K, N><<<zblocks(), nt, SM9, s>>>(rhok, phi, ts, wr, wt, tw, twh); break;
+            case 9: k_c2r_z_phi<R, K, N><<<zrows(), TZ::NT, SMZ9, s>>>(rhok, phi, ts, wr, wt, tw, twh); break;
             default: break;
         }
     }
 
     static void initial_density(cudaStream_t s, G *psi, G *rhok, TState *ts, double *part, const C *tw,
                                 const C *twh) {
-        k_density_r2c_z<R, K, N, false><<<zblocks(), TL::NT, SM, s>>>(psi, rhok, ts, part, tw, twh);
-        k_reduce_init<<<1, 256, 0, s>>>(ts, part, (int)zblocks(), double(N) * N * N);
+        k_density_r2c_z<R, K, N, false><<<zrows(), TZ::NT, SMZ, s>>>(psi, rhok, ts, part, tw, twh);
+        k_reduce_init<<<1, 256, 0, s>>>(ts, part, (int)zrows(), double(N) * N * N);
+    }
+
+    // g <- U^H g: forward FFT, drift with the conjugate tables, inverse FFT
+    static void adj_drift(cudaStream_t s, G *g, TState *ts_adj, const C *drift_conj, const C *tw,
+                          const CUtensorMap *tm, uint32_t salt) {
+        k_fft_z<R, K, N, -1><<<zrows(), TZ::NT, SMZ, s>>>(g, tw, salt);
+        pass(2, s, g, nullptr, nullptr, ts_adj, drift_conj, tw, nullptr, 0, 0, tm);
+        pass(3, s, g, nullptr, nullptr, ts_adj, drift_conj, tw, nullptr, 0, 0, tm);
+        pass(4, s, g, nullptr, nullptr, ts_adj, drift_conj, tw, nullptr, 0, 0, tm);
+        k_fft_z<R, K, N, +1><<<zrows(), TZ::NT, SMZ, s>>>(g, tw, salt ^ 0x68e31da4u);
+    }
+    // pw = phi_s[w]: real source -> half spectrum -> -1/kappa^2 -> real
+    static void poisson_of(cudaStream_t s, const R *w, R *pw, G *rhok, TState *ts_adj, const C *tw, const C *twh,
+                           const CUtensorMap *tm) {
+        k_source_r2c_z<R, K, N><<<zrows(), TZ::NT, SMZ, s>>>(w, rhok, ts_adj, tw, twh);
+        for (int p = 6; p <= 9; ++p) pass(p, s, nullptr, pw, rhok, ts_adj, nullptr, tw, twh, 0, 0, tm);
     }
 
     static void fft3d(G *data, int sign, const C *tw, cudaStream_t s) {
         const unsigned nt = TL::NT;
         if (sign < 0) {
-            k_fft_z<R, K, N, -1><<<zblocks(), nt, SM, s>>>(data, tw);
+            k_fft_z<R, K, N, -1><<<zrows(), TZ::NT, SMZ, s>>>(data, tw, 0x2545f491u);
             k_fft_yx<R, K, N, -1, 1><<<zblocks(), nt, SM, s>>>(data, N, N, nullptr, 0, tw);
             k_fft_yx<R, K, N, -1, 2><<<zblocks(), nt, SM, s>>>(data, N, N, nullptr, 0, tw);
         } else {
-            k_fft_z<R, K, N, +1><<<zblocks(), nt, SM, s>>>(data, tw);
+            k_fft_z<R, K, N, +1><<<zrows(), TZ::NT, SMZ, s>>>(data, tw, 0x2545f491u);
             k_fft_yx<R, K, N, +1, 1><<<zblocks(), nt, SM, s>>>(data, N, N, nullptr, 0, tw);
             k_fft_yx<R, K, N, +1, 2><<<zblocks(), nt, SM, s>>>(data, N, N, nullptr, 0, tw);
         }
@@ -178,18 +242,19 @@ static std::string encode_map(CUtensorMap *m, void *base, bool f64, int rank, co
     return r == CUDA_SUCCESS ? "" : "cuTensorMapEncodeTiled failed (" + std::to_string((int)r) + ")";
 }
 
-// y-pass map: [x][y][W complex] as (2W reals, N, N); x-pass map: (2*N*W reals, N)
-static std::string make_axis_maps(CUtensorMap *my, CUtensorMap *mx, void *base, bool f64, int N, int W, int L,
-                                  int boxr) {
+// y-pass map: [x][y][W complex] as (2W reals, N, N); x-pass map: (2*N*W reals, N).
+// Boxes: Ly (Lx) lines by boxr rows.
+static std::string make_axis_maps(CUtensorMap *my, CUtensorMap *mx, void *base, bool f64, int N, int W, int Ly,
+                                  int Lx, int boxr) {
     const cuuint64_t es = f64 ? 8 : 4;
     const cuuint64_t dy[3] = {cuuint64_t(2) * W, cuuint64_t(N), cuuint64_t(N)};
     const cuuint64_t sy[2] = {cuuint64_t(2) * W * es, cuuint64_t(2) * W * N * es};
-    const cuuint32_t by[3] = {cuuint32_t(2 * L), cuuint32_t(boxr), 1};
+    const cuuint32_t by[3] = {cuuint32_t(2 * Ly), cuuint32_t(boxr), 1};
     std::string e = encode_map(my, base, f64, 3, dy, sy, by);
     if (!e.empty()) return e;
     const cuuint64_t dx[2] = {cuuint64_t(2) * N * W, cuuint64_t(N)};
     const cuuint64_t sx[1] = {cuuint64_t(2) * W * N * es};
-    const cuuint32_t bx[2] = {cuuint32_t(2 * L), cuuint32_t(boxr)};
+    const cuuint32_t bx[2] = {cuuint32_t(2 * Lx), cuuint32_t(boxr)};
     return encode_map(mx, base, f64, 2, dx, sx, bx);
 }
 
@@ -197,14 +262,23 @@ static std::string make_axis_maps(CUtensorMap *my, CUtensorMap *mx, void *base, 
 static int compute_kind(int prec) { return prec == 1 ? 1 : 0; }
 static size_t storage_bytes(int prec) { return prec == 0 ? 8 : 4; }
 
-// twiddles exp(-2 pi i m / n), m < n, from long double
+// twiddles exp(-2 pi i m / n), m < n, from long double; FP32 tables pair each
+// rounded twiddle with its rounding remainder (exact - rounded): entries 2m, 2m+1
 template <typename C> static std::vector<C> twiddles(int n) {
-    std::vector<C> t(n);
+    using T = decltype(C{}.x);
+    const int per = sizeof(T) == 4 ? 2 : 1;
+    std::vector<C> t(size_t(per) * n);
     const long double twopi = 6.283185307179586476925286766559005768L;
     for (int m = 0; m < n; ++m) {
         const long double ang = -twopi * (long double)m / (long double)n;
-        t[m].x = (decltype(t[m].x))cosl(ang);
-        t[m].y = (decltype(t[m].y))sinl(ang);
+        const long double c = cosl(ang), s = sinl(ang);
+        C &h = t[size_t(per) * m];
+        h.x = (T)c;
+        h.y = (T)s;
+        if (per == 2) {
+            t[2 * size_t(m) + 1].x = (T)(c - (long double)h.x);
+            t[2 * size_t(m) + 1].y = (T)(s - (long double)h.y);
+        }
     }
     return t;
 }
@@ -224,8 +298,8 @@ static std::string get_twiddles(int n, int prec, void **out) {
         CUDA_TRY(cudaMemcpy(p, t.data(), sizeof(double2) * n, cudaMemcpyHostToDevice));
     } else {
         auto t = twiddles<float2>(n);
-        CUDA_TRY(cudaMalloc(&p, sizeof(float2) * n));
-        CUDA_TRY(cudaMemcpy(p, t.data(), sizeof(float2) * n, cudaMemcpyHostToDevice));
+        CUDA_TRY(cudaMalloc(&p, sizeof(float2) * t.size()));
+        CUDA_TRY(cudaMemcpy(p, t.data(), sizeof(float2) * t.size(), cudaMemcpyHostToDevice));
     }
     cache.push_back({dev, n, prec, p});
     *out = p;
@@ -241,6 +315,17 @@ StepEngine::~StepEngine() {
     cudaFree(drift32_);
     cudaFree(ts_);
     cudaFree(part_);
+    cudaFree(log_);
+    cudaFree(ckpt_psi_);
+    cudaFree(ckpt_phi_);
+    cudaFree(seg_psi_);
+    cudaFree(seg_phi_);
+    cudaFree(g_);
+    cudaFree(w_);
+    cudaFree(pw_);
+    cudaFree(ts_adj_);
+    cudaFree(drift64_adj_);
+    cudaFree(drift32_adj_);
 }
 
 std::string StepEngine::init(const EngineConfig &cfg, cudaStream_t stream) {
@@ -269,17 +354,14 @@ std::string StepEngine::init(const EngineConfig &cfg, cudaStream_t stream) {
     use_tma_ = N >= 128 && std::getenv("IFDM_NO_TMA") == nullptr;
     if (use_tma_) {
         const bool f64 = cfg.precision == 0;
-        const int L = cfg.precision == 1 ? 16 : 8, boxr = N < 256 ? N : 256;
-        e = make_axis_maps(&map_psi_y_, &map_psi_x_, psi_, f64, N, N, L, boxr);
-        if (e.empty()) e = make_axis_maps(&map_rho_y_, &map_rho_x_, rhok_, f64, N, nhp, L, boxr);
+        with_box2(N, cfg.precision, [&](auto box) -> std::string {
+            decltype(box)::tma_lines(tma_ly_, tma_lx_);
+            return "";
+        });
+        const int boxr = N < 256 ? N : 256;
+        e = make_axis_maps(&map_psi_y_, &map_psi_x_, psi_, f64, N, N, tma_ly_, tma_lx_, boxr);
+        if (e.empty()) e = make_axis_maps(&map_rho_y_, &map_rho_x_, rhok_, f64, N, nhp, tma_ly_, tma_lx_, boxr);
         if (!e.empty()) return e;
-        int dev = 0, sms = 0;
-        CUDA_TRY(cudaGetDevice(&dev));
-        CUDA_TRY(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));
-        const size_t tile = size_t(N) * L * (f64 ? 16 : 8);
-        const size_t work = cfg.precision == 2 ? size_t(N) * L * 16 : 0;
-        const int per_sm = (3 * tile + work + 64) * 2 <= 227 * 1024 ? 2 : 1;
-        tma_grid_ = sms * per_sm;
     }
     // max|phi| scan window of the reference: first N^3 doubles of the padded
     // [N][N][2(N/2+1)] array (the vector holds only N^3 elements,
@@ -314,6 +396,7 @@ std::string StepEngine::set_physics(double a, double rhoc) {
     ph.S2 = S2;
     ph.dt_scale = 1.0;
     ph.N = cfg_.N;
+    ph.dither = (cfg_.precision == 1 && std::getenv("IFDM_NO_DITHER") == nullptr) ? 1 : 0;
     ph.limit = 64;
     TState t;
     std::memset(&t, 0, sizeof t);
@@ -362,12 +445,11 @@ std::string StepEngine::launch_initial_density() {
         G *psi = (G *)psi_, *rhok = (G *)rhok_;
         R *phi = (R *)phi_;
         const C *tw = (const C *)tw_, *twh = (const C *)twh_;
-        if (!part_) CUDA_TRY(cudaMalloc(&part_, sizeof(double) * 3 * B::zblocks()));
+        if (!part_) CUDA_TRY(cudaMalloc(&part_, sizeof(double) * 3 * B::zrows()));
         B::initial_density(stream_, psi, rhok, ts_, part_, tw, twh);
         const CUtensorMap tm[4] = {map_psi_y_, map_psi_x_, map_rho_y_, map_rho_x_};
         for (int p = 6; p <= 9; ++p)
-            B::pass(p, stream_, psi, phi, rhok, ts_, nullptr, tw, twh, win_rows_, win_tail_, use_tma_ ? tm : nullptr,
-                    tma_grid_);
+            B::pass(p, stream_, psi, phi, rhok, ts_, nullptr, tw, twh, win_rows_, win_tail_, use_tma_ ? tm : nullptr);
         CUDA_TRY(cudaGetLastError());
         return "";
     });
@@ -394,8 +476,7 @@ std::string StepEngine::launch_passes(cudaEvent_t *ev) {
         const C *drift = compute_kind(cfg_.precision) == 0 ? (const C *)(void *)drift64_ : (const C *)(void *)drift32_;
         const CUtensorMap tm[4] = {map_psi_y_, map_psi_x_, map_rho_y_, map_rho_x_};
         for (int p = 1; p <= 9; ++p) {
-            B::pass(p, stream_, psi, phi, rhok, ts_, drift, tw, twh, win_rows_, win_tail_, use_tma_ ? tm : nullptr,
-                    tma_grid_);
+            B::pass(p, stream_, psi, phi, rhok, ts_, drift, tw, twh, win_rows_, win_tail_, use_tma_ ? tm : nullptr);
             if (ev) CUDA_TRY(cudaEventRecord(ev[p], stream_));
         }
         CUDA_TRY(cudaGetLastError());
@@ -484,6 +565,170 @@ std::string StepEngine::phi_out(double *dev_out) {
 std::string StepEngine::read_state(TState &out) {
     CUDA_TRY(cudaMemcpyAsync(&out, ts_, sizeof(TState), cudaMemcpyDeviceToHost, stream_));
     CUDA_TRY(cudaStreamSynchronize(stream_));
+    return "";
+}
+
+// ------------------------------------------------------------------ adjoint --
+std::string StepEngine::ensure_adjoint_buffers(int nsteps, int ckpt) {
+    const size_t n3 = n3_();
+    const size_t rs = storage_bytes(cfg_.precision), cs = 2 * rs;
+    const int nck = (nsteps + ckpt - 1) / ckpt;
+    if (nsteps > log_cap_) {
+        cudaFree(log_);
+        log_ = nullptr;
+        CUDA_TRY(cudaMalloc(&log_, sizeof(StepLog) * nsteps));
+        log_cap_ = nsteps;
+    }
+    if (nck > nckpt_cap_) {
+        cudaFree(ckpt_psi_);
+        cudaFree(ckpt_phi_);
+        ckpt_psi_ = ckpt_phi_ = nullptr;
+        CUDA_TRY(cudaMalloc(&ckpt_psi_, n3 * cs * nck));
+        CUDA_TRY(cudaMalloc(&ckpt_phi_, n3 * rs * nck));
+        nckpt_cap_ = nck;
+    }
+    if (ckpt > seg_cap_) {
+        cudaFree(seg_psi_);
+        cudaFree(seg_phi_);
+        seg_psi_ = seg_phi_ = nullptr;
+        CUDA_TRY(cudaMalloc(&seg_psi_, n3 * cs * ckpt));
+        CUDA_TRY(cudaMalloc(&seg_phi_, n3 * rs * ckpt));
+        seg_cap_ = ckpt;
+    }
+    if (!g_) {
+        CUDA_TRY(cudaMalloc(&g_, n3 * cs));
+        CUDA_TRY(cudaMalloc(&w_, n3 * rs));
+        CUDA_TRY(cudaMalloc(&pw_, n3 * rs));
+        CUDA_TRY(cudaMalloc(&ts_adj_, sizeof(TState)));
+        CUDA_TRY(cudaMemsetAsync(ts_adj_, 0, sizeof(TState), stream_));
+        CUDA_TRY(cudaMalloc(&drift64_adj_, sizeof(double2) * cfg_.N));
+        CUDA_TRY(cudaMalloc(&drift32_adj_, sizeof(float2) * cfg_.N));
+        if (use_tma_) {
+            const int N = cfg_.N, boxr = N < 256 ? N : 256;
+            std::string e = make_axis_maps(&map_g_y_, &map_g_x_, g_, cfg_.precision == 0, N, N, tma_ly_, tma_lx_, boxr);
+            if (!e.empty()) return e;
+        }
+    }
+    return "";
+}
+
+std::string StepEngine::record(int nsteps, double dt_scale, int ckpt) {
+    if (nsteps <= 0 || ckpt <= 0) return "record: nsteps and checkpoint interval must be positive";
+    std::string e = ensure_adjoint_buffers(nsteps, ckpt);
+    if (!e.empty()) return e;
+    const size_t n3 = n3_();
+    const size_t rs = storage_bytes(cfg_.precision), cs = 2 * rs;
+    ckpt_every_ = ckpt;
+    recorded_ = 0;
+    StepLog *lg = static_cast<StepLog *>(log_);
+    for (int n = 0; n < nsteps; ++n) {
+        if (n % ckpt == 0) {
+            const size_t k = size_t(n / ckpt);
+            CUDA_TRY(cudaMemcpyAsync((char *)ckpt_psi_ + k * n3 * cs, psi_, n3 * cs, cudaMemcpyDeviceToDevice, stream_));
+            CUDA_TRY(cudaMemcpyAsync((char *)ckpt_phi_ + k * n3 * rs, phi_, n3 * rs, cudaMemcpyDeviceToDevice, stream_));
+        }
+        e = launch_timestep(dt_scale);
+        if (!e.empty()) return e;
+        k_log_step<<<1, 1, 0, stream_>>>(ts_, lg + n);
+        e = launch_passes(nullptr);
+        if (!e.empty()) return e;
+    }
+    recorded_ = nsteps;
+    return "";
+}
+
+// one kick adjoint on g_: w, pw = phi_s[w], combine
+std::string StepEngine::adjoint_kick(void *psi, void *phi, double a, double aP, double b, double alpha,
+                                     long long tag) {
+    const size_t n3 = n3_();
+    return with_box2(cfg_.N, cfg_.precision, [&](auto box) -> std::string {
+        using B = decltype(box);
+        using C = typename B::C;
+        using G = typename B::G;
+        using R = typename B::R;
+        using K = typename B::K;
+        const C *tw = (const C *)tw_, *twh = (const C *)twh_;
+        const CUtensorMap tm[4] = {map_g_y_, map_g_x_, map_rho_y_, map_rho_x_};
+        k_adj_w<R, K><<<1184, 256, 0, stream_>>>((const G *)g_, (const G *)psi, (const R *)phi, a, b, alpha, (R *)w_,
+                                                 n3);
+        B::poisson_of(stream_, (const R *)w_, (R *)pw_, (G *)rhok_, ts_adj_, tw, twh, use_tma_ ? tm : nullptr);
+        k_adj_combine<R, K><<<1184, 256, 0, stream_>>>((G *)g_, (const G *)psi, (const R *)phi, (const R *)pw_,
+                                                       (const R *)w_, a, aP, b, alpha, n3,
+                                                       (uint32_t)(tag * 0x9e3779b9ull) ^ 0x7f4a7c15u);
+        CUDA_TRY(cudaGetLastError());
+        return "";
+    });
+}
+
+std::string StepEngine::adjoint(const double *g_final_dev, double *g0_dev) {
+    if (recorded_ <= 0) return "adjoint: no recorded steps";
+    const size_t n3 = n3_();
+    const size_t rs = storage_bytes(cfg_.precision), cs = 2 * rs;
+    const int M = recorded_, K = ckpt_every_;
+    std::vector<StepLog> lg(M);
+    CUDA_TRY(cudaMemcpyAsync(lg.data(), log_, sizeof(StepLog) * M, cudaMemcpyDeviceToHost, stream_));
+    TState fin{};
+    CUDA_TRY(cudaMemcpyAsync(&fin, ts_, sizeof(TState), cudaMemcpyDeviceToHost, stream_));
+    CUDA_TRY(cudaStreamSynchronize(stream_));
+    // natural units -> gradient with respect to the stored (scaled) field: g_s = S g
+    if (cfg_.precision == 0)
+        k_scale_in<double><<<1184, 256, 0, stream_>>>((const double2 *)g_final_dev, (double2 *)g_, S_, n3);
+    else
+        k_scale_in<float><<<1184, 256, 0, stream_>>>((const double2 *)g_final_dev, (float2 *)g_, S_, n3);
+    CUDA_TRY(cudaGetLastError());
+    // the output map: psi_out = S psi exp(-i (pendP phi + pendQ |psi|^2 - gphase))
+    std::string e = adjoint_kick(psi_, phi_, fin.pendP, fin.pendP, fin.pendQ, -fin.gphase, 1ll << 40);
+    if (!e.empty()) return e;
+    for (int seg = (M - 1) / K; seg >= 0; --seg) {
+        const int start = seg * K, end = std::min(M, start + K);
+        // replay the segment from its checkpoint, keeping every (psi_n, phi_n)
+        CUDA_TRY(cudaMemcpyAsync(psi_, (char *)ckpt_psi_ + size_t(seg) * n3 * cs, n3 * cs, cudaMemcpyDeviceToDevice,
+                                 stream_));
+        CUDA_TRY(cudaMemcpyAsync(phi_, (char *)ckpt_phi_ + size_t(seg) * n3 * rs, n3 * rs, cudaMemcpyDeviceToDevice,
+                                 stream_));
+        for (int n = start; n < end; ++n) {
+            CUDA_TRY(cudaMemcpyAsync((char *)seg_psi_ + size_t(n - start) * n3 * cs, psi_, n3 * cs,
+                                     cudaMemcpyDeviceToDevice, stream_));
+            CUDA_TRY(cudaMemcpyAsync((char *)seg_phi_ + size_t(n - start) * n3 * rs, phi_, n3 * rs,
+                                     cudaMemcpyDeviceToDevice, stream_));
+            if (n + 1 < end) {  // the last state of the segment is not needed
+                // same step counter as the forward pass, so stochastic rounding repeats exactly
+                k_replay_step<<<1, 256, 0, stream_>>>(ts_, (const StepLog *)log_ + n, cfg_.N, 0, n + 1, drift64_,
+                                                      drift32_);
+                e = launch_passes(nullptr);
+                if (!e.empty()) return e;
+            }
+        }
+        for (int n = end - 1; n >= start; --n) {
+            k_replay_step<<<1, 256, 0, stream_>>>(ts_adj_, (const StepLog *)log_ + n, cfg_.N, 1, (1ll << 32) + n,
+                                                  drift64_adj_, drift32_adj_);
+            e = with_box2(cfg_.N, cfg_.precision, [&](auto box) -> std::string {
+                using B = decltype(box);
+                using C = typename B::C;
+                using G = typename B::G;
+                const C *tw = (const C *)tw_;
+                const C *dconj = compute_kind(cfg_.precision) == 0 ? (const C *)(void *)drift64_adj_
+                                                                   : (const C *)(void *)drift32_adj_;
+                const CUtensorMap tm[4] = {map_g_y_, map_g_x_, map_rho_y_, map_rho_x_};
+                B::adj_drift(stream_, (G *)g_, ts_adj_, dconj, tw, use_tma_ ? tm : nullptr,
+                             (uint32_t)(n * 0x85ebca6bull) ^ 0xc2b2ae35u);
+                CUDA_TRY(cudaGetLastError());
+                return "";
+            });
+            if (!e.empty()) return e;
+            const StepLog &L = lg[n];
+            e = adjoint_kick((char *)seg_psi_ + size_t(n - start) * n3 * cs,
+                             (char *)seg_phi_ + size_t(n - start) * n3 * rs, L.coefP, L.coefP, L.coefQ, L.alpha, n);
+            if (!e.empty()) return e;
+        }
+    }
+    // gradient with respect to the natural-unit psi_0 = S psi_s: g0 = g_s / S
+    if (cfg_.precision == 0)
+        k_scale_out<double><<<1184, 256, 0, stream_>>>((const double2 *)g_, (double2 *)g0_dev, 1.0 / S_, n3);
+    else
+        k_scale_out<float><<<1184, 256, 0, stream_>>>((const float2 *)g_, (double2 *)g0_dev, 1.0 / S_, n3);
+    CUDA_TRY(cudaGetLastError());
+    recorded_ = 0;  // the replay consumed the state; record again before another adjoint
     return "";
 }
 

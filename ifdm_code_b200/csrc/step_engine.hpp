@@ -20,6 +20,19 @@ struct EngineConfig {
     double dt_scale = 1.0;
 };
 
+// Device buffers and constants of one box (for the batch launcher).
+struct EngineView {
+    int N, precision;
+    void *psi, *phi, *rhok;
+    const void *tw, *twh;
+    TState *ts;
+    double2 *drift64;
+    float2 *drift32;
+    Phys phys;  // dt_scale 1
+    long win_rows;
+    int win_tail;
+};
+
 // Names of the fused passes in launch order (timestep first).
 constexpr int kNumPasses = 10;
 extern const char *const kPassNames[kNumPasses];
@@ -47,6 +60,14 @@ class StepEngine {
     std::string phi_out(double *dev_out);
     // copy the TState to host (synchronous)
     std::string read_state(TState &out);
+    // Adjoint support.  record(): nsteps fixed-mode steps that keep a per-step
+    // log of the coefficients and a checkpoint of (psi, phi) every ckpt steps.
+    std::string record(int nsteps, double dt_scale, int ckpt);
+    // gradient of a real loss through the recorded steps: g_final = dL/dpsi_final
+    // (complex128, natural units, dL/dRe + i dL/dIm) -> g0 = dL/dpsi_0; both
+    // device pointers.  Leaves the context's state at an intermediate step.
+    std::string adjoint(const double *g_final_dev, double *g0_dev);
+    int recorded_steps() const { return recorded_; }
     // one step split for the native loop: timestep only / passes only
     std::string timestep_only(double dt_scale);
     std::string passes_only();
@@ -58,6 +79,9 @@ class StepEngine {
     double Phi0() const { return Phi0_; }
     size_t n3() const { return size_t(cfg_.N) * cfg_.N * cfg_.N; }
     void *psi_ptr() const { return psi_; }
+    EngineView view() const {
+        return {cfg_.N, cfg_.precision, psi_, phi_, rhok_, tw_, twh_, ts_, drift64_, drift32_, phys_, win_rows_, win_tail_};
+    }
 
   private:
     std::string launch_timestep(double dt_scale);
@@ -80,7 +104,18 @@ class StepEngine {
     // TMA descriptors of the y/x passes (psi and the half spectrum), used for N >= 128
     bool use_tma_ = false;
     CUtensorMap map_psi_y_{}, map_psi_x_{}, map_rho_y_{}, map_rho_x_{};
-    int tma_grid_ = 0;
+    int tma_ly_ = 8, tma_lx_ = 8;  // lines per TMA tile of the y and x passes (inner box extent)
+    // adjoint buffers
+    void *log_ = nullptr;  // StepLog[log_cap_]
+    int log_cap_ = 0, recorded_ = 0, ckpt_every_ = 0, nckpt_cap_ = 0, seg_cap_ = 0;
+    void *ckpt_psi_ = nullptr, *ckpt_phi_ = nullptr, *seg_psi_ = nullptr, *seg_phi_ = nullptr;
+    void *g_ = nullptr, *w_ = nullptr, *pw_ = nullptr;
+    TState *ts_adj_ = nullptr;
+    double2 *drift64_adj_ = nullptr;
+    float2 *drift32_adj_ = nullptr;
+    CUtensorMap map_g_y_{}, map_g_x_{};
+    std::string ensure_adjoint_buffers(int nsteps, int ckpt);
+    std::string adjoint_kick(void *psi, void *phi, double a, double aP, double b, double alpha, long long tag);
     int win_tail_ = 0;
 };
 

@@ -36,13 +36,16 @@ namespace ifdm {
 // R: element type in HBM, K: arithmetic type in registers and shared memory.
 // (double, double) is the FP64 drop-in, (float, float) FP32, and
 // (float, double) the mixed mode: FP32 traffic, FP64 butterflies.
-template <typename R, typename K, int N> struct Tile {
+// ZR: tiles of whole contiguous rows (z passes), which coalesce whatever the
+// line count, so L only has to fill a shared-memory phase; strided lines (y/x
+// passes) take enough lines for 128-byte segments.
+template <typename R, typename K, int N, bool ZR = false> struct Tile {
     using G = cx<R>;
     using C = cx<K>;
     static constexpr int GB = (int)sizeof(G);
     static constexpr int PH = sizeof(C) == 16 ? 8 : 16;            // threads per smem phase
-    static constexpr int LC = 128 / GB;                             // lines for 128-byte rows
-    static constexpr int E0 = Plan<N>::E * ((sizeof(C) == 16 && GB == 8 && N >= 256) ? 2 : 1);
+    static constexpr int LC = ZR ? 1 : 128 / GB;                    // lines for 128-byte rows
+    static constexpr int E0 = Plan<N>::E * ((!ZR && sizeof(C) == 16 && GB == 8 && N >= 256) ? 2 : 1);
     static constexpr int T = N / E0;                                // threads per line
     static constexpr int LT = 256 / T;                              // lines for >= 256 threads
     static constexpr int L1 = LT > LC ? LT : LC;
@@ -56,6 +59,13 @@ template <typename R, typename K, int N> struct Tile {
     static_assert(N / E0 * E0 == N, "E must divide N");
     static_assert((N / 2) / EH <= T, "half-length lines must fit the block");
 };
+template <typename R, typename K, int N> using TileZ = Tile<R, K, N, true>;
+
+// r2c / c2r post-twiddle: w^k * a (DIR -1) or conj(w^k) * a (DIR +1), table of length TN
+template <int DIR, int TN, typename C> __device__ __forceinline__ C post_tw(const C *__restrict__ tw, int k, C a) {
+    if constexpr (sizeof(C) == 16) return DIR < 0 ? cmul(__ldg(tw + k), a) : cmul(cconj(__ldg(tw + k)), a);
+    else return twmul<DIR, TN>(a, tw, k);
+}
 
 // Half-spectrum row pitch: N/2+1 rounded up so rows start on 128-byte lines.
 template <typename R> __host__ __device__ constexpr int half_pitch(int n) {
@@ -150,16 +160,21 @@ template <> __device__ __forceinline__ float2 expmi<float>(double p) {
     const double pr = p - twopi * rint(p * (1.0 / twopi));
     float s, c;
     sincosf((float)pr, &s, &c);
-    return mkc(c, -s);
+    // put the pair back on the unit circle (first-order Newton step for
+    // 1/sqrt(c^2 + s^2)): the kick must not change |psi|, and a modulus error
+    // with a sign preference would change the norm by the same amount every
+    // step instead of averaging out
+    const float f = fmaf(-0.5f, fmaf(c, c, fmaf(s, s, -1.0f)), 1.0f);
+    return mkc(c * f, -s * f);
 }
 
 // ------------------------------------------------------------- z-passes ---
 // Tiles of L consecutive rows (row r = x*N + y), row pitch N, contiguous.
 
 template <typename R, typename K, int N, int DIR>
-__global__ void __launch_bounds__(Tile<R, K, N>::NT)
-    k_fft_z(cx<R> *__restrict__ data, const cx<K> *__restrict__ tw) {
-    using TL = Tile<R, K, N>;
+__global__ void __launch_bounds__(TileZ<R, K, N>::NT)
+    k_fft_z(cx<R> *__restrict__ data, const cx<K> *__restrict__ tw, uint32_t salt) {
+    using TL = TileZ<R, K, N>;
     using C = typename TL::C;
     extern __shared__ __align__(16) unsigned char smraw[];
     C *sm = reinterpret_cast<C *>(smraw);
@@ -168,25 +183,25 @@ __global__ void __launch_bounds__(Tile<R, K, N>::NT)
     __syncthreads();
     fft_tile<C, N, TL::E, DIR, TL::L, TL::LP>(sm, tw);
     for (int f = threadIdx.x; f < TL::L * N; f += TL::NT)
-        data[base + f] = Cvt<R, K>::out(sm[(f % N) * TL::LP + f / N], 0x2545f491u, base + f);
+        data[base + f] = Cvt<R, K>::out(sm[(f % N) * TL::LP + f / N], salt, base + f);
 }
 
 // P1: kick with the merged coefficients, remove the offset c, forward FFT along z.
 template <typename R, typename K, int N>
-__global__ void __launch_bounds__(Tile<R, K, N>::NT)
+__global__ void __launch_bounds__(TileZ<R, K, N>::NT)
     k_kick_fft_z(cx<R> *__restrict__ psi, const R *__restrict__ phi, const TState *__restrict__ ts,
                  const cx<K> *__restrict__ tw) {
-    using TL = Tile<R, K, N>;
+    using TL = TileZ<R, K, N>;
     using C = typename TL::C;
     extern __shared__ __align__(16) unsigned char smraw[];
     C *sm = reinterpret_cast<C *>(smraw);
-    const double cp = ts->coefP, cq = ts->coefQ;
+    const double cp = ts->coefP, cq = ts->coefQ, alpha = ts->alpha;
     const C c0 = mkc((K)ts->cre, (K)ts->cim);
     const uint32_t salt = pass_salt(ts, 1);
     const size_t base = size_t(blockIdx.x) * TL::L * N;
     for (int f = threadIdx.x; f < TL::L * N; f += TL::NT) {
         const C v = cin<K>(psi[base + f]);
-        const double p = cp * (double)phi[base + f] + cq * (double)cnorm2(v);
+        const double p = cp * (double)phi[base + f] + cq * (double)cnorm2(v) + alpha;
         sm[(f % N) * TL::LP + f / N] = cmul(v, expmi<K>(p)) - c0;
     }
     __syncthreads();
@@ -200,10 +215,10 @@ __global__ void __launch_bounds__(Tile<R, K, N>::NT)
 // The initial pass (no IFFT) also writes per-block partial sums of psi and
 // |psi|^2 to `part` (3 doubles per block) for the offset c and the mean mu.
 template <typename R, typename K, int N, bool DO_IFFT>
-__global__ void __launch_bounds__(Tile<R, K, N>::NT)
+__global__ void __launch_bounds__(TileZ<R, K, N>::NT)
     k_density_r2c_z(cx<R> *__restrict__ psi, cx<R> *__restrict__ rhok, TState *__restrict__ ts,
                     double *__restrict__ part, const cx<K> *__restrict__ tw, const cx<K> *__restrict__ twh) {
-    using TL = Tile<R, K, N>;
+    using TL = TileZ<R, K, N>;
     using C = typename TL::C;
     constexpr int NH = N / 2 + 1;
     constexpr int NHP = half_pitch<R>(N);
@@ -263,8 +278,7 @@ __global__ void __launch_bounds__(Tile<R, K, N>::NT)
         const C zc = cconj(sm[((M - k) % M) * TL::LP + l]);
         const C e = cscale(zk + zc, K(0.5));
         const C o = cscale(zk - zc, K(0.5));
-        const C w = __ldg(tw + (k % N));
-        const C wo = cmul(w, o);  // X = e - i w o
+        const C wo = post_tw<-1, N>(tw, k % N, o);  // X = e - i w o
         const size_t gi = (row0 + l) * NHP + k;
         rhok[gi] = Cvt<R, K>::out(mkc(e.x + wo.y, e.y - wo.x), salt2, gi);
     }
@@ -274,10 +288,10 @@ __global__ void __launch_bounds__(Tile<R, K, N>::NT)
 // over the reference's scan window (rows below win_rows, plus win_tail
 // elements of row win_rows; see the timestep kernel).
 template <typename R, typename K, int N>
-__global__ void __launch_bounds__(Tile<R, K, N>::NT)
+__global__ void __launch_bounds__(TileZ<R, K, N>::NT)
     k_c2r_z_phi(const cx<R> *__restrict__ rhok, R *__restrict__ phi, TState *__restrict__ ts, long win_rows,
                 int win_tail, const cx<K> *__restrict__ tw, const cx<K> *__restrict__ twh) {
-    using TL = Tile<R, K, N>;
+    using TL = TileZ<R, K, N>;
     using C = typename TL::C;
     constexpr int NHP = half_pitch<R>(N);
     constexpr int M = N / 2;
@@ -299,17 +313,17 @@ __global__ void __launch_bounds__(Tile<R, K, N>::NT)
         const C xk = xs[k * TL::LP + l];
         const C xc = cconj(xs[(M - k) * TL::LP + l]);
         const C e = xk + xc;
-        const C d = cmul(cconj(__ldg(tw + k)), xk - xc);
+        const C d = post_tw<+1, N>(tw, k, xk - xc);
         sm[k * TL::LP + l] = mkc(e.x - d.y, e.y + d.x);
     }
     __syncthreads();
     fft_tile<C, M, TL::EH, +1, TL::L, TL::LP>(sm, twh);
     const K *smr = reinterpret_cast<const K *>(sm);
-    const K inv = K(1.0 / ((double)N * N * N));
+    constexpr KSplit<K> inv(1.0 / ((double)N * N * N));
     double mx = 0.0;
     for (int f = threadIdx.x; f < TL::L * N; f += TL::NT) {
         const int l = f / N, n = f % N;
-        const R v = Cvt<R, K>::outr(smr[2 * ((n >> 1) * TL::LP + l) + (n & 1)] * inv, salt, row0 * N + f);
+        const R v = Cvt<R, K>::outr(mulk(smr[2 * ((n >> 1) * TL::LP + l) + (n & 1)], inv.hi, inv.lo), salt, row0 * N + f);
         phi[row0 * N + f] = v;
         const long row = (long)(row0 + l);
         if (row < win_rows || (row == win_rows && n < win_tail)) mx = fmax(mx, (double)fabs(v));
@@ -375,7 +389,9 @@ __global__ void __launch_bounds__(Tile<R, K, N>::NT)
         ts->cnext_im = ts->cim + (double)sm[0].y * inv;
     }
     const int y = int(q / N), z = int(q % N);
-    const C lf = cscale(cmul(__ldg(drift + y), __ldg(drift + z)), K(1.0 / ((double)N * N * N)));
+    constexpr KSplit<K> inv3(1.0 / ((double)N * N * N));
+    const C dyz = cmul(__ldg(drift + y), __ldg(drift + z));
+    const C lf = mkc(mulk(dyz.x, inv3.hi, inv3.lo), mulk(dyz.y, inv3.hi, inv3.lo));
     for (int n = threadIdx.x / TL::L; n < N; n += TL::NT / TL::L)
         sm[n * TL::LP + l] = cmul(sm[n * TL::LP + l], cmul(lf, __ldg(drift + n)));
     __syncthreads();
@@ -429,11 +445,13 @@ __global__ void k_psi_out(const cx<R> *__restrict__ psi, const R *__restrict__ p
                           int which, double S, double2 *__restrict__ out, size_t n) {
     const double cp = which == 1 ? ts->snapP : (which == 2 ? ts->pendP : 0.0);
     const double cq = which == 1 ? ts->snapQ : (which == 2 ? ts->pendQ : 0.0);
+    // undo the accumulated dither phase (psi is stored as exp(-i g) psi)
+    const double g = which == 1 ? ts->gphase_prev : ts->gphase;
     for (size_t i = size_t(blockIdx.x) * blockDim.x + threadIdx.x; i < n; i += size_t(gridDim.x) * blockDim.x) {
         const cx<R> v = psi[i];
         double2 w = make_double2((double)v.x, (double)v.y);
-        if (which) {
-            const double p = cp * (double)phi[i] + cq * (w.x * w.x + w.y * w.y);
+        if (which || g != 0.0) {
+            const double p = cp * (double)phi[i] + cq * (w.x * w.x + w.y * w.y) - g;
             double s, c;
             sincos(p, &s, &c);
             w = make_double2(w.x * c + w.y * s, w.y * c - w.x * s);

@@ -41,7 +41,7 @@ __device__ __constant__ double c_gk_wg[5] = {
     0.219086362515982043995534934228163, 0.269266719309996355091226921569469,
     0.295524224714752870173892994651338};
 
-__device__ void qk21(int n, double H0, double Om, double a, double b, double *res, double *abserr, double *resasc) {
+static __device__ void qk21(int n, double H0, double Om, double a, double b, double *res, double *abserr, double *resasc) {
     const double c = 0.5 * (a + b), h = 0.5 * (b - a);
     const double fc = qk_integrand(n, c, H0, Om);
     double kron = fc * c_gk_wk[10], gauss = 0.0, sabs = fabs(kron);
@@ -82,7 +82,7 @@ __device__ void qk21(int n, double H0, double Om, double a, double b, double *re
 
 #define IFDM_QLIMIT 64
 // Returns 0 on success, 1 when the interval limit was reached.
-__device__ int qags_dev(int n, double H0, double Om, double a, double b, int limit, double *result) {
+static __device__ int qags_dev(int n, double H0, double Om, double a, double b, int limit, double *result) {
     double r0, e0, s0;
     qk21(n, H0, Om, a, b, &r0, &e0, &s0);
     if ((e0 <= 1e-10 * fabs(r0) && e0 != s0) || e0 == 0.0) {
@@ -117,7 +117,7 @@ __device__ __forceinline__ double bits_to_double(unsigned long long b) { return 
 
 // After the initial density pass: partial sums (3 per block, fixed order) ->
 // first offset c = mean psi_s and the conserved mean mu = <|psi_s|^2>.
-__global__ void k_reduce_init(TState *__restrict__ ts, const double *__restrict__ part, int nblocks, double n3) {
+static __global__ void k_reduce_init(TState *__restrict__ ts, const double *__restrict__ part, int nblocks, double n3) {
     __shared__ double red[3][256];
     double a = 0, b = 0, c = 0;
     for (int i = threadIdx.x; i < nblocks; i += blockDim.x) {
@@ -144,9 +144,9 @@ __global__ void k_reduce_init(TState *__restrict__ ts, const double *__restrict_
     }
 }
 
-// The timestep.  drift64/drift32: tables exp(-i s kappa_i^2), i < N.
-__global__ void k_timestep(TState *__restrict__ ts, Phys ph, double2 *__restrict__ drift64,
-                           float2 *__restrict__ drift32) {
+// The timestep.  drift64/drift32: tables exp(-i s kappa_i^2), i < N.  Run by
+// one block: thread 0 does the scalar work, all threads fill the tables.
+__device__ __forceinline__ void timestep_body(TState *ts, const Phys &ph, double2 *drift64, float2 *drift32) {
     __shared__ double s_drift;
     if (threadIdx.x == 0) {
         const double maxphi = ph.Phi0 * bits_to_double(ts->maxphi_bits);
@@ -189,8 +189,23 @@ __global__ void k_timestep(TState *__restrict__ ts, Phys ph, double2 *__restrict
         ts->pendP = hp;
         ts->pendQ = hq;
         ts->drift_s = ph.kin * iKE;
-        ts->cre = ts->cnext_re;
-        ts->cim = ts->cnext_im;
+        // global-phase dither (FP32 mode): psi is stored as exp(-i gphase) psi
+        // and this step's kick adds alpha, a pseudo-random phase in [0, 2 pi)
+        // from the step count, so consecutive steps round different numbers;
+        // the offset c (a mean of psi) rotates with it
+        double alpha = 0.0;
+        if (ph.dither) {
+            const unsigned long long h = (unsigned long long)ts->steps * 0x9e3779b97f4a7c15ull + 0x632be59bd9b4e019ull;
+            const unsigned long long m = (h ^ (h >> 31)) * 0xbf58476d1ce4e5b9ull;
+            alpha = 6.283185307179586476925286766559 * (double)((m ^ (m >> 29)) >> 11) * 0x1.0p-53;
+        }
+        double sa, ca;
+        sincos(alpha, &sa, &ca);
+        ts->alpha = alpha;
+        ts->gphase_prev = ts->gphase;
+        ts->gphase = fmod(ts->gphase + alpha, 6.283185307179586476925286766559);
+        ts->cre = ts->cnext_re * ca + ts->cnext_im * sa;
+        ts->cim = ts->cnext_im * ca - ts->cnext_re * sa;
         ts->steps += 1;
         s_drift = ph.kin * iKE;
     }
@@ -206,6 +221,11 @@ __global__ void k_timestep(TState *__restrict__ ts, Phys ph, double2 *__restrict
         drift64[i] = make_double2(cs, -sn);
         drift32[i] = make_float2((float)cs, (float)-sn);
     }
+}
+
+static __global__ void k_timestep(TState *__restrict__ ts, Phys ph, double2 *__restrict__ drift64,
+                           float2 *__restrict__ drift32) {
+    timestep_body(ts, ph, drift64, drift32);
 }
 
 }  // namespace ifdm

@@ -87,3 +87,30 @@ __device__ __forceinline__ void prefetch_tmap(const CUtensorMap *map) {
 }
 
 }  // namespace ifdm
+
+namespace ifdm {
+
+// Per-thread asynchronous global->shared copies (LDGSTS).  Each thread can
+// place its element anywhere in the tile, so a transposing, padded layout is
+// filled without a register round trip.  Completion is per thread and per
+// commit group; a __syncthreads() after wait_group makes the tile visible.
+__device__ __forceinline__ void cp_async4(void *dst, const void *src) {
+    asm volatile("cp.async.ca.shared.global [%0], [%1], 4;" ::"r"(smem_u32(dst)), "l"(src) : "memory");
+}
+__device__ __forceinline__ void cp_async8(void *dst, const void *src) {
+    asm volatile("cp.async.ca.shared.global [%0], [%1], 8;" ::"r"(smem_u32(dst)), "l"(src) : "memory");
+}
+__device__ __forceinline__ void cp_async16(void *dst, const void *src) {
+    asm volatile("cp.async.cg.shared.global [%0], [%1], 16;" ::"r"(smem_u32(dst)), "l"(src) : "memory");
+}
+template <int BYTES> __device__ __forceinline__ void cp_async(void *dst, const void *src) {
+    if constexpr (BYTES == 16) cp_async16(dst, src);
+    else if constexpr (BYTES == 8) cp_async8(dst, src);
+    else cp_async4(dst, src);
+}
+__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;" ::: "memory"); }
+template <int PENDING> __device__ __forceinline__ void cp_async_wait() {
+    asm volatile("cp.async.wait_group %0;" ::"n"(PENDING) : "memory");
+}
+
+}  // namespace ifdm

@@ -22,12 +22,16 @@ namespace ifdm {
 
 // R: element type in HBM (TMA landing ring), K: arithmetic type.  When they
 // differ (mixed mode) the landing slot is converted into a separate FP64
-// compute tile and freed before the transform; rows are then 64 bytes.
-template <typename R, typename K, int N> struct TmaTile {
+// compute tile and freed before the transform.
+// AXIS 2 tiles carry the x passes (two transforms each), AXIS 1 the y passes.
+template <typename R, typename K, int N, int AXIS = 1> struct TmaTile {
     using G = cx<R>;
     using C = cx<K>;
     static constexpr bool SPLIT = !std::is_same<R, K>::value;
-    static constexpr int L = SPLIT ? 8 : 128 / (int)sizeof(G);  // lines per tile
+    // lines per tile: 128-byte rows.  (Measured at 512^3: 8-line x tiles for
+    // FP32, which avoid the spills of 1024 threads at 64 registers, ran P3/P7
+    // slower, 0.97/0.57 ms against 0.82/0.39 ms.)
+    static constexpr int L = SPLIT ? 8 : 128 / (int)sizeof(G);
     static constexpr int E = Plan<N>::E;
     static constexpr int T = N / E;
     static constexpr int NT = L * T;
@@ -41,10 +45,10 @@ template <typename R, typename K, int N> struct TmaTile {
 };
 
 template <typename R, typename K, int N, int AXIS, int MODE, int DIR>
-__global__ void __launch_bounds__(TmaTile<R, K, N>::NT, 1)
+__global__ void __launch_bounds__(TmaTile<R, K, N, AXIS>::NT, 1)
     k_yx_tma(const __grid_constant__ CUtensorMap map, cx<R> *__restrict__ data, int W, int VW, int ntiles,
              TState *__restrict__ ts, int pass, const cx<K> *__restrict__ drift, const cx<K> *__restrict__ tw) {
-    using TL = TmaTile<R, K, N>;
+    using TL = TmaTile<R, K, N, AXIS>;
     using G = cx<R>;
     using C = cx<K>;
     constexpr int L = TL::L, T = TL::T, ST = TL::STAGES;
@@ -112,7 +116,9 @@ __global__ void __launch_bounds__(TmaTile<R, K, N>::NT, 1)
                     ts->cnext_im = ts->cim + (double)v[0].y * inv;
                 }
                 const int y = int(g / N), z = int(g % N);
-                const C lf = cscale(cmul(__ldg(drift + y), __ldg(drift + z)), K(1.0 / ((double)N * N * N)));
+                constexpr KSplit<K> inv3(1.0 / ((double)N * N * N));
+                const C dyz = cmul(__ldg(drift + y), __ldg(drift + z));
+                const C lf = mkc(mulk(dyz.x, inv3.hi, inv3.lo), mulk(dyz.y, inv3.hi, inv3.lo));
 #pragma unroll
                 for (int b = 0; b < E / RL; ++b)
 #pragma unroll

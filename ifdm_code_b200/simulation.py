@@ -14,7 +14,7 @@ import ctypes as C
 import numpy as np
 
 from . import _lib
-from ._lib import IfdmError, Params, State
+from ._lib import BatchTuning, IfdmError, Params, State
 
 
 def _check(lib, h, rc: int) -> int:
@@ -97,6 +97,21 @@ class Simulation:
         self._c(self.lib.ifdm_get_psi(self.h, out.ctypes.data_as(C.c_void_p)))
         return out
 
+    def get_psi_into(self, tensor) -> None:
+        """psi after the latest step into a contiguous complex128 CUDA tensor."""
+        self._c(self.lib.ifdm_get_psi(self.h, C.c_void_p(tensor.data_ptr())))
+
+    def record_steps(self, nsteps: int, dt_scale: float = 1.0, checkpoint_every: int = 20) -> None:
+        """nsteps fixed-mode steps that keep what ``adjoint`` needs."""
+        self._c(self.lib.ifdm_record_steps(self.h, nsteps, dt_scale, checkpoint_every))
+
+    def adjoint(self, g_final, g0) -> None:
+        """dL/dpsi_final -> dL/dpsi_0 through the recorded steps (complex128
+        numpy arrays or CUDA tensors, dL/dRe + i dL/dIm)."""
+        def ptr(a):
+            return C.c_void_p(a.data_ptr()) if hasattr(a, "data_ptr") else a.ctypes.data_as(C.c_void_p)
+        self._c(self.lib.ifdm_adjoint(self.h, ptr(g_final), ptr(g0)))
+
     def get_phi(self) -> np.ndarray:
         out = np.empty((self.N,) * 3, dtype=np.float64)
         self._c(self.lib.ifdm_get_phi(self.h, out.ctypes.data_as(C.c_void_p)))
@@ -157,3 +172,82 @@ def fft3d_(tensor, sign: int, compute: str | None = None) -> None:
 
 def supported_res(res: int, precision: str = "fp64") -> bool:
     return bool(_lib.load_library().ifdm_supported_res(res, {"fp64": 0, "fp32": 1, "mixed": 2}[precision]))
+
+
+class Batch:
+    """Several Simulations (res 16..128, one device, one precision) advanced
+    together: one replay of a captured CUDA graph per ``step`` call, in which
+    the boxes of each grid size share one persistent kernel (or one launch per
+    phase, whichever ``tune`` found faster).  Each box keeps its own state and
+    is read through its Simulation as usual."""
+
+    def __init__(self, sims: list[Simulation]):
+        self.lib = _lib.load_library()
+        self.sims = list(sims)
+        arr = (C.c_void_p * len(self.sims))(*[s.h for s in self.sims])
+        h = C.c_void_p()
+        rc = self.lib.ifdm_batch_create(arr, len(self.sims), C.byref(h))
+        self.h = h.value
+        if rc < 0:
+            msg = self.lib.ifdm_batch_last_error(self.h) if self.h else b""
+            self.close()
+            raise IfdmError(rc, msg.decode() if msg else "")
+
+    def _c(self, rc: int) -> int:
+        if rc < 0:
+            msg = self.lib.ifdm_batch_last_error(self.h)
+            raise IfdmError(rc, msg.decode() if msg else "")
+        return rc
+
+    def _dts(self, dt_scale):
+        if np.isscalar(dt_scale):
+            dt_scale = [float(dt_scale)] * len(self.sims)
+        if len(dt_scale) != len(self.sims):
+            raise ValueError("one dt_scale per box")
+        return (C.c_double * len(self.sims))(*[float(x) for x in dt_scale])
+
+    def step(self, nsteps: int, dt_scale=1.0) -> None:
+        """nsteps fixed-mode steps of every box (asynchronous)."""
+        self._c(self.lib.ifdm_batch_step(self.h, nsteps, self._dts(dt_scale)))
+
+    def tune(self, trial_steps: int, dt_scale=1.0) -> dict:
+        t = BatchTuning()
+        self._c(self.lib.ifdm_batch_tune(self.h, trial_steps, self._dts(dt_scale), C.byref(t)))
+        return self._tuning_dict(t)
+
+    def get_tuning(self) -> dict:
+        t = BatchTuning()
+        self._c(self.lib.ifdm_batch_get_tuning(self.h, C.byref(t)))
+        return self._tuning_dict(t)
+
+    def set_tuning(self, mode: int = 0, blocks_per_sm: int = 2, group: int = 0, plan=(0,) * 6) -> None:
+        t = BatchTuning(mode, blocks_per_sm, group, (C.c_int * 6)(*plan), 0.0)
+        self._c(self.lib.ifdm_batch_set_tuning(self.h, C.byref(t)))
+
+    @staticmethod
+    def _tuning_dict(t) -> dict:
+        return {"mode": t.mode, "blocks_per_sm": t.blocks_per_sm, "group": t.group, "plan": list(t.plan),
+                "ms_per_step": t.ms_per_step}
+
+    def info(self) -> dict:
+        items, grid = C.c_longlong(), C.c_int()
+        self._c(self.lib.ifdm_batch_info(self.h, C.byref(items), C.byref(grid)))
+        return {"items_per_step": items.value, "grid": grid.value}
+
+    def synchronize(self) -> None:
+        self._c(self.lib.ifdm_batch_synchronize(self.h))
+
+    def close(self) -> None:
+        if getattr(self, "h", None):
+            self.lib.ifdm_batch_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        self.close()
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *exc):
+        self.close()
+

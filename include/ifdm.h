@@ -136,6 +136,55 @@ int ifdm_profile_passes(ifdm_ctx *ctx, int nsteps, double dt_scale, double *ms_o
 /* Algorithmic HBM bytes one step moves, per pass (same order as above). */
 int ifdm_pass_bytes(ifdm_ctx *ctx, double *bytes_out, int cap);
 
+/* Adjoint of the split step (no counterpart in the reference, which has no
+ * derivatives).  ifdm_record_steps runs nsteps fixed-mode steps like
+ * ifdm_step and keeps what the adjoint needs: the coefficients of every step
+ * and a checkpoint of (psi, phi) every checkpoint_every steps.
+ * ifdm_adjoint then maps g_final = dL/dRe psi_final + i dL/dIm psi_final (psi
+ * as ifdm_get_psi returns it) to the same derivative with respect to the psi
+ * the recording started from, replaying each segment forward from its
+ * checkpoint and sweeping it backwards: g' = U^H g, w = Im(conj(g') K psi),
+ * g = exp(i theta) g' + 2 (a phi_s[w] + b w) psi.  The Delta-t schedule is
+ * the recorded one.  Both arrays are complex128 N^3, host or device.  The
+ * replay overwrites the context's state: set a psi again before stepping. */
+int ifdm_record_steps(ifdm_ctx *ctx, int nsteps, double dt_scale, int checkpoint_every);
+int ifdm_adjoint(ifdm_ctx *ctx, const double *g_final, double *g0);
+
+/* Batches: many independent boxes advanced together (no counterpart in the
+ * reference, which runs one box per MPI job).  A batch groups contexts made
+ * by ifdm_create on one device with one precision, res 16, 32, 48, 64, 96 or
+ * 128 (sizes may differ), each with a state (ifdm_set_psi, ifdm_load_ic or
+ * ifdm_load_snapshot).  ifdm_batch_step advances every box by nsteps
+ * fixed-mode steps, box b with step scale dt_scale[b] (as ifdm_step), in one
+ * replay of one captured CUDA graph: the boxes of each grid size share one
+ * persistent kernel (or, the other schedule, one launch per phase), sizes run
+ * side by side, with the same passes and tile shapes as a one-box run of
+ * these sizes.  Contexts are read as usual afterwards (ifdm_get_psi,
+ * ifdm_get_state) and must outlive the batch.  ifdm_batch_tune times launch
+ * shapes on trial_steps steps (saving and restoring every box's state) and
+ * keeps the fastest: the schedule, CTAs per SM, the group size of the item
+ * order (all boxes in lock step, or a few at a time for L2 reuse) and the
+ * radix plan of each grid size. */
+typedef struct ifdm_batch ifdm_batch;
+typedef struct ifdm_batch_tuning {
+    int mode;           /* 0: one persistent kernel per grid size, 1: one launch per phase and size */
+    int blocks_per_sm;  /* persistent CTAs per SM */
+    int group;          /* boxes per group of the item order, 0 = all boxes */
+    int plan[6];        /* radix-plan variant (0, 1) for res 16, 32, 48, 64, 96, 128 */
+    double ms_per_step; /* ifdm_batch_tune: measured time of one batch step */
+} ifdm_batch_tuning;
+int ifdm_batch_create(ifdm_ctx *const *ctxs, int n, ifdm_batch **out);
+int ifdm_batch_step(ifdm_batch *b, int nsteps, const double *dt_scale);
+int ifdm_batch_tune(ifdm_batch *b, int trial_steps, const double *dt_scale, ifdm_batch_tuning *out);
+int ifdm_batch_get_tuning(ifdm_batch *b, ifdm_batch_tuning *out);
+int ifdm_batch_set_tuning(ifdm_batch *b, const ifdm_batch_tuning *t);
+/* Wait for the batch; IFDM_ERR_DEVICE if a dependency wait gave up. */
+int ifdm_batch_synchronize(ifdm_batch *b);
+/* Work items of one batch step and the persistent CTAs of all sizes. */
+int ifdm_batch_info(ifdm_batch *b, long long *items_per_step, int *grid);
+const char *ifdm_batch_last_error(const ifdm_batch *b);
+void ifdm_batch_destroy(ifdm_batch *b);
+
 /* Device-pointer transforms on the caller's stream (cudaStream_t as void*).
  * In-place unnormalised 3-D complex FFT of data[n][n][n] (complex128 when
  * precision == IFDM_FP64, complex64 otherwise; IFDM_MIXED computes in FP64);

@@ -1,0 +1,118 @@
+"""Adjoint split step against central finite differences (needs a B200).
+
+The loss is the L2 distance between the final log-density and a target
+log-density from a run of another seed.  Directional derivatives of the loss
+along seeded random unit directions in the scaled field psi/S (S^2 = rho_c/m,
+so |psi/S| ~ 1) are compared with <g, d> from the adjoint.  The finite
+differences always come from FP64 forward runs: a reduced-precision forward
+run cannot resolve a loss change of ~1e-11 (its own rounding noise is larger),
+so the mixed-precision gradient is checked against the FP64 finite differences
+and against the FP64 adjoint.
+
+The adjoint treats the step schedule as fixed (it depends on max reductions),
+so every case runs where each step is limited by the kinetic criterion, which
+depends on a alone; `_assert_kinetic_schedule` checks that.
+"""
+
+import numpy as np
+import pytest
+
+import ifdm_code_b200 as ifdm
+from ifdm_code_b200.autograd import evolve
+from ifdm_code_b200.synthetic_ic import zeldovich_psi
+
+pytestmark = pytest.mark.gpu
+
+MFDM, XMAX, A0 = 2.5e-24, 5.0, 1.0 / 51.0
+RHOC = 3.51059e10
+S = np.sqrt(RHOC / (MFDM * 1.783e-36 / 1.989e30))
+
+
+def _loss(psi, target_logrho):
+    import torch
+
+    return ((torch.log(psi.abs() ** 2 / S**2) - target_logrho) ** 2).mean()
+
+
+def _target(n, nsteps, dt_scale, prec):
+    import torch
+
+    tgt = torch.from_numpy(zeldovich_psi(n, seed=12)).cuda()
+    sim = ifdm.Simulation(MFDM, 0.0, XMAX, n, precision=prec)
+    with torch.no_grad():
+        t_out = evolve(tgt, sim, A0, nsteps, dt_scale, 7)
+    sim.close()
+    return torch.log(t_out.abs() ** 2 / S**2)
+
+
+def _assert_kinetic_schedule(n, nsteps, dt_scale):
+    psi0 = zeldovich_psi(n, seed=11)
+    with ifdm.Simulation(MFDM, 0.0, XMAX, n) as sim:
+        sim.set_psi(psi0, A0)
+        for _ in range(nsteps):
+            sim.step(1, dt_scale)
+            assert sim.state()["criterion"] == 3, "a step was not limited by the kinetic criterion"
+
+
+def _gradient(n, nsteps, dt_scale, ckpt, prec, target):
+    import torch
+
+    psi0 = torch.from_numpy(zeldovich_psi(n, seed=11)).cuda()
+    sim = ifdm.Simulation(MFDM, 0.0, XMAX, n, precision=prec)
+    x = psi0.clone().requires_grad_(True)
+    _loss(evolve(x, sim, A0, nsteps, dt_scale, ckpt), target).backward()
+    sim.close()
+    return psi0, x.grad.detach() * S  # gradient in the scaled field psi/S
+
+
+def _fd_check(n, nsteps, dt_scale, ckpt, prec, tol, ndir):
+    import torch
+
+    target = _target(n, nsteps, dt_scale, "fp64")
+    psi0, g = _gradient(n, nsteps, dt_scale, ckpt, prec, target)
+    sim = ifdm.Simulation(MFDM, 0.0, XMAX, n, precision="fp64")
+    rng = np.random.default_rng(3)
+    eps = 1e-3
+    for _ in range(ndir):
+        d = rng.standard_normal((n, n, n)) + 1j * rng.standard_normal((n, n, n))
+        d = torch.from_numpy(d / np.linalg.norm(d)).cuda()
+        with torch.no_grad():
+            lp = _loss(evolve(psi0 + eps * S * d, sim, A0, nsteps, dt_scale, ckpt), target).item()
+            lm = _loss(evolve(psi0 - eps * S * d, sim, A0, nsteps, dt_scale, ckpt), target).item()
+        fd = (lp - lm) / (2 * eps)
+        adj = float(torch.sum(g.real * d.real + g.imag * d.imag).item())
+        err = abs(fd - adj) / max(abs(fd), abs(adj))
+        assert err <= tol, (fd, adj, err)
+    sim.close()
+
+
+@pytest.mark.parametrize("prec,tol", [("fp64", 2e-5), ("mixed", 2e-3)])
+def test_adjoint_matches_finite_differences(prec, tol):
+    n, nsteps, C, ckpt = 64, 24, 0.05, 7  # 4 segments, the last one partial
+    _assert_kinetic_schedule(n, nsteps, C)
+    _fd_check(n, nsteps, C, ckpt, prec, tol, ndir=16)
+
+
+def test_adjoint_128_200_steps_mixed():
+    """128^3, 200 steps, mixed forward, checkpoints every 20 steps, 16 directions.
+
+    The step scale keeps every step kinetic-limited: with the scale that
+    reaches a = 0.5 in 200 steps (0.22) the potential criterion takes over
+    before the end, and a schedule that depends on max|phi| is not what the
+    adjoint differentiates.
+    """
+    n, nsteps, C, ckpt = 128, 200, 0.05, 20
+    _assert_kinetic_schedule(n, nsteps, C)
+    _fd_check(n, nsteps, C, ckpt, "mixed", 5e-3, ndir=16)
+
+
+def test_reduced_precision_adjoint_close_to_fp64():
+    n, nsteps, C = 64, 16, 0.05
+    target = _target(n, nsteps, C, "fp64")
+    grads = {}
+    for prec in ("fp64", "mixed", "fp32"):
+        _, g = _gradient(n, nsteps, C, 5, prec, target)
+        grads[prec] = g.cpu().numpy()
+    for prec, tol in (("mixed", 1e-4), ("fp32", 1e-3)):
+        e = np.linalg.norm(grads[prec] - grads["fp64"]) / np.linalg.norm(grads["fp64"])
+        assert e <= tol, (prec, e)

@@ -1,0 +1,125 @@
+"""Batches of uneven boxes against the same boxes run one at a time (needs a B200).
+
+A batch runs the same fused passes with the same tile shapes, step salts and
+radix plans as a one-box run of each size, so with the default plans every
+box up to 96^3 must come out bit for bit equal to ifdm_step on that box alone,
+in both schedules (persistent kernels, one launch per phase); one-box runs at
+128^3 take the TMA passes, whose roundings may differ.  The alternative radix
+plans change only the order of FFT additions: those runs are compared within
+a rounding tolerance.
+"""
+
+import numpy as np
+import pytest
+
+import ifdm_code_b200 as ifdm
+from ifdm_code_b200._lib import IfdmError
+from ifdm_code_b200.synthetic_ic import zeldovich_psi
+
+pytestmark = pytest.mark.gpu
+
+XMAX, A0 = 5.0, 1.0 / 51.0
+SIZES = [32, 48, 64, 96, 32, 64, 16, 128]
+
+
+def _boxes(prec, sizes=SIZES):
+    rng = np.random.default_rng(7)
+    sims, psis, dts = [], [], []
+    for i, n in enumerate(sizes):
+        m = float(rng.uniform(1e-24, 5e-24))
+        psi = zeldovich_psi(n, xmax=XMAX, seed=500 + i, a=A0, mfdm=m)
+        sim = ifdm.Simulation(m, 0.0, XMAX, n, precision=prec)
+        sim.set_psi(psi, A0)
+        sims.append(sim)
+        psis.append(psi)
+        dts.append(float(rng.uniform(0.02, 0.08)))
+    return sims, psis, dts
+
+
+def _one_at_a_time(prec, psis, sizes, dts, nsteps):
+    out = []
+    rng = np.random.default_rng(7)
+    for i, n in enumerate(sizes):
+        m = float(rng.uniform(1e-24, 5e-24))
+        rng.uniform(0.02, 0.08)
+        with ifdm.Simulation(m, 0.0, XMAX, n, precision=prec) as sim:
+            sim.set_psi(psis[i], A0)
+            sim.step(nsteps, dts[i])
+            out.append((sim.get_psi(), sim.state()))
+    return out
+
+
+@pytest.mark.parametrize("prec", ["mixed", "fp64", "fp32"])
+@pytest.mark.parametrize("mode", [0, 1])
+def test_batch_equals_one_at_a_time(prec, mode):
+    nsteps = 12
+    sims, psis, dts = _boxes(prec)
+    ref = _one_at_a_time(prec, psis, SIZES, dts, nsteps)
+    with ifdm.Batch(sims) as b:
+        b.set_tuning(mode=mode, blocks_per_sm=2, group=3 if mode == 0 else 0)
+        b.step(nsteps // 2, dts)
+        b.step(nsteps - nsteps // 2, dts)  # a second replay continues the state
+        b.synchronize()
+        for i, sim in enumerate(sims):
+            got = sim.get_psi()
+            st = sim.state()
+            assert st["steps"] == ref[i][1]["steps"] and st["a"] == ref[i][1]["a"]
+            if SIZES[i] < 128:
+                assert np.array_equal(got, ref[i][0]), (SIZES[i], np.abs(got - ref[i][0]).max())
+            else:  # one-box runs at 128 take the TMA register-chain passes: same sums, other roundings
+                e = np.linalg.norm(got - ref[i][0]) / np.linalg.norm(ref[i][0])
+                assert e < {"fp64": 1e-12, "mixed": 1e-5, "fp32": 1e-4}[prec], (SIZES[i], e)
+    for s in sims:
+        s.close()
+
+
+def test_batch_alternative_plans_and_tuner():
+    nsteps = 8
+    prec = "mixed"
+    sims, psis, dts = _boxes(prec)
+    ref = _one_at_a_time(prec, psis, SIZES, dts, nsteps)
+    with ifdm.Batch(sims) as b:
+        t = b.tune(3, dts)  # times candidates on saved-and-restored states
+        assert t["ms_per_step"] > 0 and t["mode"] in (0, 1)
+        b.set_tuning(mode=0, blocks_per_sm=2, group=0, plan=(1,) * 6)
+        b.step(nsteps, dts)
+        b.synchronize()
+        for i, sim in enumerate(sims):
+            got = sim.get_psi()
+            e = np.linalg.norm(got - ref[i][0]) / np.linalg.norm(ref[i][0])
+            assert e < 1e-5, (SIZES[i], e)
+    for s in sims:
+        s.close()
+
+
+def test_batch_tune_leaves_state():
+    nsteps = 6
+    sims, psis, dts = _boxes("mixed", SIZES[:4])
+    ref = _one_at_a_time("mixed", psis, SIZES[:4], dts, nsteps)
+    with ifdm.Batch(sims) as b:
+        t = b.tune(2, dts)
+        b.set_tuning(mode=t["mode"], blocks_per_sm=t["blocks_per_sm"], group=t["group"], plan=(0,) * 6)
+        b.step(nsteps, dts)
+        b.synchronize()
+        for i, sim in enumerate(sims):
+            assert np.array_equal(sim.get_psi(), ref[i][0]), SIZES[i]
+    for s in sims:
+        s.close()
+
+
+def test_batch_errors():
+    a = ifdm.Simulation(2.5e-24, 0.0, XMAX, 32, precision="mixed")
+    c = ifdm.Simulation(2.5e-24, 0.0, XMAX, 32, precision="fp64")
+    big = ifdm.Simulation(2.5e-24, 0.0, XMAX, 256, precision="mixed")
+    with pytest.raises(IfdmError) as e:
+        ifdm.Batch([a, c])
+    assert e.value.code == -5
+    with pytest.raises(IfdmError) as e:
+        ifdm.Batch([a, big])
+    assert e.value.code == -5
+    with ifdm.Batch([a]) as b:
+        with pytest.raises(IfdmError) as e:
+            b.step(1, 1.0)  # no wave function yet
+        assert e.value.code == -6
+    for s in (a, c, big):
+        s.close()

@@ -181,6 +181,28 @@ def cpu_baseline_port(N: int, psi0, dt_scale: float):
             "sample": f"1 leap-frog step of the {N}^3 workload ({dt:.1f} s)"}
 
 
+# Kernels of the 512^3 passes whose DRAM traffic per launch was captured with
+# ncu (summary and command in profiles/fp32_512_step_kernels.md).
+PROFILED_KERNEL = {("fp32", "P1"): "k_kick_fft_z<float,float,512>",
+                   ("fp32", "P2"): "k_yx_tma<float,float,512,1,0,(int)-1>",
+                   ("fp32", "P3"): "k_yx_tma<float,float,512,2,1,0>",
+                   ("fp32", "P5"): "k_density_r2c_z_pipe<float,512>"}
+
+
+def profiled_traffic(prec: str, pass_name: str, N: int):
+    """DRAM bytes read + written per launch by the pass's kernel, from the
+    committed ncu summary (512^3 only), else None."""
+    key = PROFILED_KERNEL.get((prec, pass_name.split("_")[0]))
+    path = os.path.join(os.path.dirname(os.path.abspath(__file__)), "profiles", "fp32_512_step_kernels.md")
+    if N != 512 or key is None or not os.path.exists(path):
+        return None
+    for line in open(path):
+        f = line.split()
+        if len(f) == 4 and f[0] == "traffic" and f[1] == prec and f[2] == key:
+            return float(f[3])
+    return None
+
+
 def run_ours(args):
     import numpy as np
     import torch
@@ -316,14 +338,15 @@ def run_ours(args):
     fp64_value = vals["fp64"]
     e2e_value = world * cells * K / e2e_s
 
-    def roofline(r):
+    def roofline(r, prec):
         names = list(r["prof"].keys())
         ms = [r["prof"][n] for n in names]
         i = max(range(1, len(ms)), key=lambda j: ms[j])
         achieved = r["bytes"][i] / (ms[i] / 1e3) / 1e9
         step_bytes = sum(r["bytes"])
         return {"bound": "hbm", "kernel": names[i], "achieved": round(achieved, 1), "peak": hbm, "unit": "GB/s",
-                "frac": round(achieved / hbm, 4), "traffic": None, "peak_kind": peak_kind,
+                "frac": round(achieved / hbm, 4), "traffic": profiled_traffic(prec, names[i], N),
+                "algorithmic_bytes": r["bytes"][i], "peak_kind": peak_kind,
                 "step_bytes_per_cell": step_bytes / cells,
                 "step_achieved_gbs": round(step_bytes / (sum(ms) / 1e3) / 1e9, 1),
                 "passes_ms": {n: round(v, 4) for n, v in zip(names, ms)},
@@ -349,11 +372,11 @@ def run_ours(args):
                    "res": N, "parallelism": f"replicas x{world}" if world > 1 else "1 box",
                    "l2": "inputs larger than L2 (psi fp32 = %.1f GB)" % (8 * cells / 1e9)},
         "paths": {p: {"value": vals[p], "ms_per_step": res[p]["ms"] / K, "over_fp64": vals[p] / fp64_value,
-                      "roofline": roofline(res[p]), "clocks": res[p]["clocks"]} for p in res},
+                      "roofline": roofline(res[p], p), "clocks": res[p]["clocks"]} for p in res},
         "precision": prec_report,
         "adjoint": adj,
         "batch": batch,
-        "roofline": roofline(res[head]),
+        "roofline": roofline(res[head], head),
         "e2e": {"value": e2e_value, "unit": "cell-steps/s", "h2d_bytes_per_step": 16 * cells / K,
                 "d2h_bytes_per_step": 16 * cells / K,
                 "note": f"set_psi from pinned host complex128, {K} steps, get_psi to pinned host, per step = /K"},
@@ -406,6 +429,12 @@ def run_batch(args, prec, device):
     t_batch = time.perf_counter() - t0
     out_batch = [sim.get_psi() for sim in sims]
     info = b.info()
+    # the same schedule with the default radix plans: the arithmetic of the one-box runs
+    b.set_tuning(mode=tuning["mode"], blocks_per_sm=tuning["blocks_per_sm"], group=tuning["group"], plan=(0,) * 6)
+    reset()
+    b.step(K, dts)
+    b.synchronize()
+    out_default = [sim.get_psi() for sim in sims]
     b.close()
     reset()
     t0 = time.perf_counter()
@@ -413,7 +442,15 @@ def run_batch(args, prec, device):
         sim.step(K, dt)
         sim.synchronize()
     t_single = time.perf_counter() - t0
-    diff = max(float(np.linalg.norm(sim.get_psi() - o) / np.linalg.norm(o)) for sim, o in zip(sims, out_batch))
+    single = [sim.get_psi() for sim in sims]
+
+    def max_rel(xs, ys):
+        return max(float(np.linalg.norm(x - y) / np.linalg.norm(y)) for x, y in zip(xs, ys))
+
+    def max_rel_rho(xs, ys):
+        return max(float(np.linalg.norm(np.abs(x) ** 2 - np.abs(y) ** 2) / np.linalg.norm(np.abs(y) ** 2))
+                   for x, y in zip(xs, ys))
+
     a_end = min(sim.state()["a"] for sim in sims)
     for sim in sims:
         sim.close()
@@ -421,7 +458,11 @@ def run_batch(args, prec, device):
     return {"path": prec, "boxes": len(sizes), "sizes": {"32": 32, "48": 32, "64": 24, "96": 8}, "steps": K,
             "value": cells * K / t_batch, "unit": "cell-steps/s", "batch_s": t_batch, "one_at_a_time_s": t_single,
             "speedup": t_single / t_batch, "one_at_a_time_value": cells * K / t_single,
-            "max_rel_l2_vs_one_at_a_time": diff, "min_a_end": a_end, "tuning": tuning,
+            "psi_rel_l2_vs_one_at_a_time": {"default_plans": max_rel(out_default, single),
+                                            "tuned_plans": max_rel(out_batch, single)},
+            "density_rel_l2_vs_one_at_a_time": {"default_plans": max_rel_rho(out_default, single),
+                                                "tuned_plans": max_rel_rho(out_batch, single)},
+            "min_a_end": a_end, "tuning": tuning,
             "items_per_step": info["items_per_step"], "persistent_ctas": info["grid"],
             "note": "wall clock around one graph replay (state reset between runs, graph captured beforehand)"}
 

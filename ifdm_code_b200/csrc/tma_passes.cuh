@@ -28,10 +28,10 @@ template <typename R, typename K, int N, int AXIS = 1> struct TmaTile {
     using G = cx<R>;
     using C = cx<K>;
     static constexpr bool SPLIT = !std::is_same<R, K>::value;
-    // lines per tile: 128-byte rows.  (Measured at 512^3: 8-line x tiles for
-    // FP32, which avoid the spills of 1024 threads at 64 registers, ran P3/P7
-    // slower, 0.97/0.57 ms against 0.82/0.39 ms.)
-    static constexpr int L = SPLIT ? 8 : 128 / (int)sizeof(G);
+    // lines per tile: 128-byte rows, except for the FP32 x passes at N = 512,
+    // whose two chained transforms with compensated twiddles spill heavily at
+    // the 64-register cap of 1024 threads; 8 lines (512 threads) do not spill
+    static constexpr int L = (SPLIT || (AXIS == 2 && sizeof(G) == 8 && N >= 512)) ? 8 : 128 / (int)sizeof(G);
     static constexpr int E = Plan<N>::E;
     static constexpr int T = N / E;
     static constexpr int NT = L * T;

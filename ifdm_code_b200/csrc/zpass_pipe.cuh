@@ -16,7 +16,7 @@ namespace ifdm {
 template <typename R, int N> struct ZPipe {
     using TL = Tile<R, R, N>;
     using C = cx<R>;
-    static constexpr int L = TL::L, LP = TL::LP, NT = TL::NT, E = TL::E;
+    static constexpr int L = TL::L, LP = TL::LP, E = TL::E, NT = TL::NT, EH = TL::EH;
     static constexpr size_t TILE = size_t(N) * LP * sizeof(C);  // one slot
     static constexpr size_t SMEM5 = 2 * TILE;
     static_assert(SMEM5 <= 227 * 1024, "shared memory per block");
@@ -32,7 +32,6 @@ __global__ void __launch_bounds__(ZPipe<R, N>::NT, 1)
     k_density_r2c_z_pipe(cx<R> *__restrict__ psi, cx<R> *__restrict__ rhok, TState *__restrict__ ts,
                          const cx<R> *__restrict__ tw, const cx<R> *__restrict__ twh, int ntiles) {
     using ZP = ZPipe<R, N>;
-    using TL = typename ZP::TL;
     using C = cx<R>;
     constexpr int L = ZP::L, LP = ZP::LP, NT = ZP::NT;
     constexpr int NH = N / 2 + 1, NHP = half_pitch<R>(N), M = N / 2;
@@ -78,7 +77,7 @@ __global__ void __launch_bounds__(ZPipe<R, N>::NT, 1)
             smr[2 * ((n >> 1) * LP + l) + (n & 1)] = rho[e];
         }
         __syncthreads();
-        fft_tile<C, M, TL::EH, -1, L, LP>(sm, twh);
+        fft_tile<C, M, ZP::EH, -1, L, LP>(sm, twh);
         for (int f = tid; f < L * NH; f += NT) {
             const int l = f / NH, k = f % NH;
             const C zk = sm[(k % M) * LP + l];

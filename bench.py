@@ -210,18 +210,10 @@ def run_ours(args):
     import ifdm_code_b200 as ifdm
     from ifdm_code_b200.synthetic_ic import zeldovich_psi
 
-    world = int(os.environ.get("WORLD_SIZE", "1"))
-    rank = int(os.environ.get("RANK", "0"))
-    local = int(os.environ.get("LOCAL_RANK", "0"))
-    dist = None
-    if world > 1:
-        import datetime
+    from ifdm_code_b200.replicas import Replicas
 
-        import torch.distributed as dist
-
-        torch.cuda.set_device(local)
-        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=600))
-    torch.cuda.set_device(local)
+    rep_ = Replicas("nccl")
+    world, rank, local = rep_.world, rep_.rank, rep_.local
     N = args.res
     K, W = args.steps, args.warmup
     C = dt_scale_for(N)
@@ -229,17 +221,8 @@ def run_ours(args):
     peaks, peak_kind = measured_peaks()
     hbm = float(peaks["hbm_gbs"])
 
-    def barrier():
-        if dist:
-            dist.barrier()
-        torch.cuda.synchronize()
-
-    def max_over_ranks(v):
-        if not dist:
-            return v
-        t = torch.tensor([v], dtype=torch.float64, device="cuda")
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        return float(t.item())
+    barrier = rep_.barrier
+    max_over_ranks = rep_.max
 
     res = {}
     for prec in ("fp64", "mixed", "fp32"):
@@ -314,7 +297,8 @@ def run_ours(args):
         adj = {"path": head, "steps": ka, "checkpoint_every": 20, "forward_s": t_fwd, "backward_s": t_bwd,
                "adjoint_over_forward": t_bwd / t_fwd}
 
-    batch = run_batch(args, head, local) if args.batch_steps > 0 else None
+    # the headline path, and mixed (whose boxes equal their one-at-a-time runs bit for bit)
+    batch = {p: run_batch(args, p, local) for p in dict.fromkeys([head, "mixed"])} if args.batch_steps > 0 else None
 
     # end to end through the C ABI with host buffers (pinned)
     pin_in = torch.from_numpy(psi0.view(np.float64)).pin_memory()
@@ -385,8 +369,7 @@ def run_ours(args):
     }
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         out["cpu_baseline"] = cpu_baseline_port(N, psi0, C)
-    if dist:
-        dist.destroy_process_group()
+    rep_.close()
     if rank == 0:
         print(json.dumps(out))
 
@@ -394,9 +377,10 @@ def run_ours(args):
 def run_batch(args, prec, device):
     """96 realisations of uneven sizes (32 at 32^3, 32 at 48^3, 24 at 64^3, 8 at
     96^3), each with its own seed and mfdm ~ U[1e-24, 5e-24] eV, g = 0, K steps
-    with per-box step scales that reach a = 0.5 at step 500: one tuned graph
-    launch per K steps against the same runs one at a time (each run's K
-    steps, then a synchronize)."""
+    with per-box step scales under which 500 kinetic-limited steps would reach
+    a = 0.5 (potential-limited steps advance less): one tuned graph launch per
+    K steps against the same runs one at a time (each run's K steps, then a
+    synchronize)."""
     import numpy as np
 
     import ifdm_code_b200 as ifdm

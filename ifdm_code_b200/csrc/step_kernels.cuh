@@ -199,9 +199,21 @@ __global__ void __launch_bounds__(TileZ<R, K, N>::NT)
     const C c0 = mkc((K)ts->cre, (K)ts->cim);
     const uint32_t salt = pass_salt(ts, 1);
     const size_t base = size_t(blockIdx.x) * TL::L * N;
-    for (int f = threadIdx.x; f < TL::L * N; f += TL::NT) {
-        const C v = cin<K>(psi[base + f]);
-        const double p = cp * (double)phi[base + f] + cq * (double)cnorm2(v) + alpha;
+    // all of this thread's loads first (PER of psi and of phi in flight), then the kicks
+    constexpr int PER = TL::L * N / TL::NT;
+    static_assert(PER * TL::NT == TL::L * N, "whole rows per thread block");
+    typename TL::G g[PER];
+    R ph[PER];
+#pragma unroll
+    for (int i = 0; i < PER; ++i) {
+        g[i] = psi[base + threadIdx.x + i * TL::NT];
+        ph[i] = phi[base + threadIdx.x + i * TL::NT];
+    }
+#pragma unroll
+    for (int i = 0; i < PER; ++i) {
+        const int f = threadIdx.x + i * TL::NT;
+        const C v = cin<K>(g[i]);
+        const double p = cp * (double)ph[i] + cq * (double)cnorm2(v) + alpha;
         sm[(f % N) * TL::LP + f / N] = cmul(v, expmi<K>(p)) - c0;
     }
     __syncthreads();
@@ -229,7 +241,14 @@ __global__ void __launch_bounds__(TileZ<R, K, N>::NT)
     const size_t base = row0 * N;
     const uint32_t salt = pass_salt(ts, 5), salt2 = pass_salt(ts, 10);
     if (DO_IFFT) {
-        for (int f = threadIdx.x; f < TL::L * N; f += TL::NT) sm[(f % N) * TL::LP + f / N] = cin<K>(psi[base + f]);
+        typename TL::G g[TL::E];  // all of this thread's loads first
+#pragma unroll
+        for (int i = 0; i < TL::E; ++i) g[i] = psi[base + threadIdx.x + i * TL::NT];
+#pragma unroll
+        for (int i = 0; i < TL::E; ++i) {
+            const int f = threadIdx.x + i * TL::NT;
+            sm[(f % N) * TL::LP + f / N] = cin<K>(g[i]);
+        }
         __syncthreads();
         fft_tile<C, N, TL::E, +1, TL::L, TL::LP>(sm, tw);
     }
@@ -300,11 +319,23 @@ __global__ void __launch_bounds__(TileZ<R, K, N>::NT)
     C *xs = sm + M * TL::LP;  // X_k rows k = 0..M staged after the Z tile
     const size_t row0 = size_t(blockIdx.x) * TL::L;
     const uint32_t salt = pass_salt(ts, 9);
-    for (int f = threadIdx.x; f < TL::L * (M + 1); f += TL::NT) {
-        const int l = f / (M + 1), k = f % (M + 1);
-        C x = cin<K>(rhok[(row0 + l) * NHP + k]);
-        if (k == 0 || k == M) x.y = K(0);  // c2r ignores these imaginary parts
-        xs[k * TL::LP + l] = x;
+    // all of this thread's loads first, then the shared-memory stores
+    constexpr int PER = (TL::L * (M + 1) + TL::NT - 1) / TL::NT;
+    typename TL::G g[PER];
+#pragma unroll
+    for (int i = 0; i < PER; ++i) {
+        const int f = threadIdx.x + i * TL::NT;
+        if (f < TL::L * (M + 1)) g[i] = rhok[(row0 + f / (M + 1)) * NHP + f % (M + 1)];
+    }
+#pragma unroll
+    for (int i = 0; i < PER; ++i) {
+        const int f = threadIdx.x + i * TL::NT;
+        if (f < TL::L * (M + 1)) {
+            const int l = f / (M + 1), k = f % (M + 1);
+            C x = cin<K>(g[i]);
+            if (k == 0 || k == M) x.y = K(0);  // c2r ignores these imaginary parts
+            xs[k * TL::LP + l] = x;
+        }
     }
     __syncthreads();
     // Z'_k = (X_k + conj X_{M-k}) + i conj(w^k) (X_k - conj X_{M-k}), k < M

@@ -4,7 +4,8 @@ A batch runs the same fused passes with the same tile shapes, step salts and
 radix plans as a one-box run of each size, in both schedules (persistent
 kernels, one launch per phase).  The same sums compiled into another kernel may
 round differently in the last bit, so FP64 and FP32 boxes are compared within
-a rounding tolerance after 12 steps; mixed-precision boxes up to 96^3 must be
+a rounding tolerance after 12 steps (in FP32 a potential-limited step size
+follows max|phi| to ~1e-7); mixed-precision boxes up to 96^3 must be
 bit for bit equal (their stored values are FP64 results rounded
 stochastically to FP32, which a last-bit difference almost never changes;
 one-box runs at 128^3 take the TMA passes).  The alternative radix plans
@@ -68,14 +69,14 @@ def test_batch_equals_one_at_a_time(prec, mode):
             st = sim.state()
             assert st["steps"] == ref[i][1]["steps"]
             # potential-limited steps take max|phi|, whose last bits may differ
-            assert abs(st["a"] - ref[i][1]["a"]) <= 1e-12 * ref[i][1]["a"]
+            assert abs(st["a"] - ref[i][1]["a"]) <= {"fp64": 1e-12, "mixed": 0.0, "fp32": 1e-5}[prec] * ref[i][1]["a"]
             e = np.linalg.norm(got - ref[i][0]) / np.linalg.norm(ref[i][0])
             if prec == "mixed" and SIZES[i] < 128:
                 # FP64 arithmetic rounded stochastically to FP32 at the stores: a last-bit
                 # difference of the FP64 intermediates almost never changes a stored value
                 assert np.array_equal(got, ref[i][0]), (SIZES[i], e)
             else:  # the same sums compiled in another kernel may round differently in the last bit
-                assert e < {"fp64": 1e-12, "mixed": 1e-5, "fp32": 1e-5}[prec], (SIZES[i], e)
+                assert e < {"fp64": 1e-12, "mixed": 1e-5, "fp32": 1e-4}[prec], (SIZES[i], e)
     for s in sims:
         s.close()
 

@@ -29,12 +29,15 @@ __device__ __forceinline__ double2 mkc(double a, double b) { return make_double2
 __device__ __forceinline__ float2 mkc(float a, float b) { return make_float2(a, b); }
 __device__ __forceinline__ double2 operator+(double2 a, double2 b) { return mkc(a.x + b.x, a.y + b.y); }
 __device__ __forceinline__ double2 operator-(double2 a, double2 b) { return mkc(a.x - b.x, a.y - b.y); }
-__device__ __forceinline__ float2 operator+(float2 a, float2 b) { return mkc(a.x + b.x, a.y + b.y); }
-__device__ __forceinline__ float2 operator-(float2 a, float2 b) { return mkc(a.x - b.x, a.y - b.y); }
+// FP32 complex sums on the paired FP32 pipe of sm_100 (one instruction per
+// complex add; each component rounds exactly like the scalar add)
+__device__ __forceinline__ float2 operator+(float2 a, float2 b) { return __fadd2_rn(a, b); }
+__device__ __forceinline__ float2 operator-(float2 a, float2 b) { return __fadd2_rn(a, make_float2(-b.x, -b.y)); }
 template <typename C> __device__ __forceinline__ C cmul(C a, C b) {
     return mkc(a.x * b.x - a.y * b.y, a.x * b.y + a.y * b.x);
 }
 template <typename C, typename S> __device__ __forceinline__ C cscale(C a, S s) { return mkc(a.x * s, a.y * s); }
+__device__ __forceinline__ float2 cscale(float2 a, float s) { return __fmul2_rn(a, make_float2(s, s)); }
 template <typename C> __device__ __forceinline__ C cconj(C a) { return mkc(a.x, -a.y); }
 // multiply by -i (DIR = -1) or +i (DIR = +1)
 template <int DIR, typename C> __device__ __forceinline__ C mul_i(C a) {

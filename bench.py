@@ -167,6 +167,64 @@ def power_spectrum(rho, nbins: int = 24):
     return sums[cnt > 0] / cnt[cnt > 0]
 
 
+def g_for_phase(N: int, psi0, dt_scale: float, phase: float) -> float:
+    """Self-interaction g [eV cm^3] whose kick turns the densest cell of psi0 by
+    `phase` radians in the first step: that turn is dt_QI (g/hbar) max|psi|^2
+    with dt_QI = integral of da/(H a^4) over the first, kinetic-limited step
+    (src/CosmoBEC_MPI.cpp:30-68, src/struct3D.h:127-146), linear in g."""
+    import math
+
+    import numpy as np
+    from scipy.integrate import quad
+
+    if phase <= 0:
+        return 0.0
+    m2Mpc, cm2Mpc, s2Myr = 3.086e22, 3.086e24, 60.0 * 60.0 * 24.0 * 365.0 * 1e6
+    hbar = 6.58211928e-16 / s2Myr
+    c = 2.99792458e8 / m2Mpc * s2Myr
+    H0, Om = 0.677 * 100 * s2Myr / m2Mpc * 1e3, 0.276
+    dx = 2.0 * (XMAX / 0.677) / N
+    dt_ke = 4.0 / (3.0 * math.pi) * (MFDM / c**2) / hbar * dx**2 * A0 * A0
+
+    def H(a):
+        return H0 * math.sqrt(Om / a**3 + 1 - Om)
+
+    da = H(A0) * A0 * dt_ke * dt_scale
+    dt_qi = quad(lambda a: 1.0 / (H(a) * a**4), A0, A0 + da, epsabs=0, epsrel=1e-12)[0]
+    max_rho = float(np.max(np.abs(psi0) ** 2))
+    return phase * hbar * cm2Mpc**3 / (dt_qi * max_rho)
+
+
+def precision_report(N: int, g: float, nsteps: int, device: int, seed: int = 0) -> dict:
+    """Density after nsteps steps (step scale reaching a = 0.5 at step 1000,
+    500... as for the benchmark) in mixed and FP32 against FP64 from the same
+    IC: relative L2 of the density, norm drift, P(k) ratio per k-bin."""
+    import numpy as np
+
+    import ifdm_code_b200 as ifdm
+    from ifdm_code_b200.synthetic_ic import zeldovich_psi
+
+    C = dt_scale_for(N, nsteps)
+    psi0 = zeldovich_psi(N, xmax=XMAX, seed=seed, a=A0, mfdm=MFDM)
+    rho = {}
+    for prec in ("fp64", "mixed", "fp32"):
+        with ifdm.Simulation(MFDM, g, XMAX, N, precision=prec, device=device) as sim:
+            sim.set_psi(psi0, A0)
+            sim.step(nsteps, C)
+            rho[prec] = np.abs(sim.get_psi()) ** 2
+            a_end = sim.state()["a"]
+    pk_ref = power_spectrum(rho["fp64"])
+    out = {"res": N, "g": g, "steps": nsteps, "dt_scale": C, "a_end": a_end}
+    for prec in ("mixed", "fp32"):
+        r, ref = rho[prec], rho["fp64"]
+        ratio = power_spectrum(r) / pk_ref
+        out[prec] = {"density_relL2": float(np.linalg.norm(r - ref) / np.linalg.norm(ref)),
+                     "norm_drift": float(r.sum() / ref.sum() - 1.0),
+                     "pk_ratio_max_dev": float(np.max(np.abs(ratio - 1.0))),
+                     "pk_ratio_per_bin": [round(float(x), 9) for x in ratio]}
+    return out
+
+
 def cpu_baseline_port(N: int, psi0, dt_scale: float):
     """The oracle (C restatement, OpenMP on every host core) for one step at N^3."""
     from oracle import Oracle, OracleArgs
@@ -223,10 +281,20 @@ def run_ours(args):
 
     barrier = rep_.barrier
     max_over_ranks = rep_.max
+    # self-interaction of the 512^3 precision config: ~0.1 rad per step at the densest cell
+    G = g_for_phase(N, psi0, C, args.g_phase)
+    turn = None
+    if G:
+        with ifdm.Simulation(MFDM, G, XMAX, N, device=local) as sim:  # check: the first step's turn
+            sim.set_psi(psi0, A0)
+            sim.step(1, C)
+            st = sim.state()
+        s2Myr = 60.0 * 60.0 * 24.0 * 365.0 * 1e6
+        turn = st["dt_QI"] * (G / 3.086e24 ** 3) / (6.58211928e-16 / s2Myr) * st["max_rho"]
 
     res = {}
     for prec in ("fp64", "mixed", "fp32"):
-        sim = ifdm.Simulation(MFDM, 0.0, XMAX, N, precision=prec, device=local)
+        sim = ifdm.Simulation(MFDM, G, XMAX, N, precision=prec, device=local)
         sim.set_psi(psi0, A0)
         sim.step(W, C)
         sim.synchronize()
@@ -261,6 +329,7 @@ def run_ours(args):
                 "density_relL2": float(np.linalg.norm(rho - ref) / np.linalg.norm(ref)),
                 "norm_drift": float(rho.sum() / ref.sum() - 1.0),
                 "pk_ratio_max_dev": float(np.max(np.abs(pk / pk_ref - 1.0))),
+                "pk_ratio_per_bin": [round(float(x), 9) for x in pk / pk_ref],
                 "a_end": res[prec]["a_end"],
             }
             del res[prec]["rho"]
@@ -275,7 +344,7 @@ def run_ours(args):
     adj = None
     if args.adjoint_steps > 0:
         ka = args.adjoint_steps
-        sim = ifdm.Simulation(MFDM, 0.0, XMAX, N, precision=head, device=local)
+        sim = ifdm.Simulation(MFDM, G, XMAX, N, precision=head, device=local)
         sim.set_psi(psi0, A0)
         sim.synchronize()
         t0 = time.perf_counter()
@@ -298,12 +367,15 @@ def run_ours(args):
                "adjoint_over_forward": t_bwd / t_fwd}
 
     # the headline path, and mixed (whose boxes equal their one-at-a-time runs bit for bit)
+    # the 256^3, g = 0 precision config (1000 steps), reported beside the headline
+    prec256 = precision_report(256, 0.0, 1000, local) if (args.precision_steps > 0 and N == 512) else None
+
     batch = {p: run_batch(args, p, local) for p in dict.fromkeys([head, "mixed"])} if args.batch_steps > 0 else None
 
     # end to end through the C ABI with host buffers (pinned)
     pin_in = torch.from_numpy(psi0.view(np.float64)).pin_memory()
     pin_out = torch.empty_like(pin_in).pin_memory()
-    sim = ifdm.Simulation(MFDM, 0.0, XMAX, N, precision=head, device=local)
+    sim = ifdm.Simulation(MFDM, G, XMAX, N, precision=head, device=local)
     sim.set_psi(pin_in.numpy().view(np.complex128), A0)
     sim.step(W, C)
     sim.synchronize()
@@ -351,13 +423,16 @@ def run_ours(args):
         "dtype": {"mixed": "f32 storage / f64 arithmetic", "fp32": "f32", "fp64": "f64"}[head],
         "path": head,
         "data": "synthetic",
-        "config": {"workload": f"{N}^3 leap-frog step, xmax=5 Mpc/h, mfdm=2.5e-24 eV, g=0, z=50 Zel'dovich IC, "
+        "config": {"workload": f"{N}^3 leap-frog step, xmax=5 Mpc/h, mfdm=2.5e-24 eV, g={G:.4e} eV cm^3 "
+                               f"({args.g_phase} rad/step at the densest cell), z=50 Zel'dovich IC, "
                                f"fixed-step dt_scale={C:.4f} (1000 steps to a=0.5)",
+                   "g_eV_cm3": G, "g_turn_first_step_rad": turn,
                    "res": N, "parallelism": f"replicas x{world}" if world > 1 else "1 box",
                    "l2": "inputs larger than L2 (psi fp32 = %.1f GB)" % (8 * cells / 1e9)},
         "paths": {p: {"value": vals[p], "ms_per_step": res[p]["ms"] / K, "over_fp64": vals[p] / fp64_value,
                       "roofline": roofline(res[p], p), "clocks": res[p]["clocks"]} for p in res},
         "precision": prec_report,
+        "precision_256_g0": prec256,
         "adjoint": adj,
         "batch": batch,
         "roofline": roofline(res[head], head),
@@ -470,6 +545,7 @@ def run_reference(args):
     W = 1
     with tempfile.TemporaryDirectory() as d:
         psi0 = zeldovich_psi(N, xmax=XMAX, seed=0, a=A0, mfdm=MFDM)
+        G = g_for_phase(N, psi0, dt_scale_for(N), args.g_phase)  # the same self-interaction as the GPU arm
         xm = XMAX / 0.677
         x = xm / N - xm + np.arange(N) * (2 * xm / N)
         with open(os.path.join(d, "output1.dat"), "wb") as f:
@@ -481,7 +557,7 @@ def run_reference(args):
         env = dict(os.environ, IFDM_SHIM_TIMING=tf)
         # rerun from output1.dat; t_write larger than the run so only the last
         # step writes (that step is not timed)
-        cmd = [binary, str(MFDM), "0", str(XMAX), str(N), "1000000", str(1 + W + K + 1), "1", d + "/", d + "/", "1"]
+        cmd = [binary, str(MFDM), repr(G), str(XMAX), str(N), "1000000", str(1 + W + K + 1), "1", d + "/", d + "/", "1"]
         subprocess.run(cmd, env=env, capture_output=True, text=True, check=True)
         ts = [float(v) for v in open(tf).read().split()]
     starts = ts[0::2]
@@ -493,8 +569,9 @@ def run_reference(args):
         "impl": "reference", "metric": METRIC, "value": value, "unit": "cell-steps/s", "n_gpus": 0,
         "steps": len(dts), "warmup": W, "ms_per_step": sec * 1e3, "higher_is_better": True, "scaling": "weak",
         "vs_baseline": None, "dtype": "f64", "data": "synthetic",
-        "config": {"workload": f"{N}^3 leap-frog step (reference loop, rerun from a synthetic snapshot)",
-                   "res": N},
+        "config": {"workload": f"{N}^3 leap-frog step (reference loop, rerun from a synthetic snapshot), "
+                               f"g={G:.4e} eV cm^3 ({args.g_phase} rad/step at the densest cell)",
+                   "res": N, "g_eV_cm3": G},
         "cpu_baseline": {"value": value, "unit": "cell-steps/s", "cores": cores, "kind": "reference",
                          "sample": f"{len(dts)} timed steps after {W} warm-up at {N}^3; FFTs on {cores} OpenMP "
                                    "threads (shim), pointwise loops on 1 thread as one MPI rank runs them"},
@@ -529,6 +606,8 @@ def main():
     ap.add_argument("--profile", action="store_true", help="plain W+K steps of --precision (for ncu)")
     ap.add_argument("--precision", choices=["fp32", "fp64", "mixed"], default="mixed")
     ap.add_argument("--adjoint-steps", type=int, default=40, help="steps of the adjoint timing (0 skips it)")
+    ap.add_argument("--g-phase", type=float, default=0.1,
+                    help="self-interaction: radians per step at the densest cell (0: g = 0)")
     ap.add_argument("--batch-steps", type=int, default=500, help="steps of the 96-box batch timing (0 skips it)")
     ap.add_argument("--precision-steps", type=int, default=1000,
                     help="steps of the precision gate (density error vs FP64); 0 skips it")

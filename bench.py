@@ -195,6 +195,32 @@ def g_for_phase(N: int, psi0, dt_scale: float, phase: float) -> float:
     return phase * hbar * cm2Mpc**3 / (dt_qi * max_rho)
 
 
+def calibrate_g(args) -> None:
+    """Print the g of the self-interaction config: the g=0 FP64 run of the
+    benchmark (1000 steps to a = 0.5) gives, per step, the turn per unit g of
+    the densest cell, dt_QI max|psi|^2 / hbar; g is set so that the largest of
+    these over the run is --g-phase radians."""
+    import ifdm_code_b200 as ifdm
+    from ifdm_code_b200.synthetic_ic import zeldovich_psi
+
+    N = args.res
+    C = dt_scale_for(N)
+    psi0 = zeldovich_psi(N, xmax=XMAX, seed=0, a=A0, mfdm=MFDM)
+    s2Myr = 60.0 * 60.0 * 24.0 * 365.0 * 1e6
+    hbar, cm2Mpc = 6.58211928e-16 / s2Myr, 3.086e24
+    peak, at = 0.0, 0
+    with ifdm.Simulation(MFDM, 0.0, XMAX, N) as sim:
+        sim.set_psi(psi0, A0)
+        for n in range(args.precision_steps):
+            sim.step(1, C)
+            st = sim.state()
+            per_g = st["dt_QI"] * st["max_rho"] / hbar / cm2Mpc ** 3  # radians per unit g [eV cm^3]
+            if per_g > peak:
+                peak, at = per_g, n
+    print(json.dumps({"res": N, "steps": args.precision_steps, "peak_turn_per_unit_g": peak, "at_step": at,
+                      "g_eV_cm3": args.g_phase / peak}))
+
+
 def precision_report(N: int, g: float, nsteps: int, device: int, seed: int = 0) -> dict:
     """Density after nsteps steps (step scale reaching a = 0.5 at step 1000,
     500... as for the benchmark) in mixed and FP32 against FP64 from the same
@@ -367,6 +393,25 @@ def run_ours(args):
                "adjoint_over_forward": t_bwd / t_fwd}
 
     # the headline path, and mixed (whose boxes equal their one-at-a-time runs bit for bit)
+    # cuFFT through torch.fft, a reference point only: one forward + inverse 3-D
+    # c2c of psi (a step needs this pair, a real-to-complex pair for the
+    # Poisson solve, the kick, the drift and the reductions)
+    fft_ref = {}
+    for name, dt in (("complex64", torch.complex64), ("complex128", torch.complex128)):
+        x = torch.from_numpy(psi0).to(device=f"cuda:{local}", dtype=dt)
+        for _ in range(2):
+            x = torch.fft.ifftn(torch.fft.fftn(x))
+        ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        torch.cuda.synchronize()
+        ev0.record()
+        for _ in range(5):
+            x = torch.fft.ifftn(torch.fft.fftn(x))
+        ev1.record()
+        torch.cuda.synchronize()
+        fft_ref[name + "_fft_pair_ms"] = ev0.elapsed_time(ev1) / 5
+        del x
+        torch.cuda.empty_cache()
+
     # the 256^3, g = 0 precision config (1000 steps), reported beside the headline
     prec256 = precision_report(256, 0.0, 1000, local) if (args.precision_steps > 0 and N == 512) else None
 
@@ -433,6 +478,7 @@ def run_ours(args):
                       "roofline": roofline(res[p], p), "clocks": res[p]["clocks"]} for p in res},
         "precision": prec_report,
         "precision_256_g0": prec256,
+        "cufft_reference": fft_ref,
         "adjoint": adj,
         "batch": batch,
         "roofline": roofline(res[head], head),
@@ -604,6 +650,7 @@ def main():
     ap.add_argument("--res", type=int, default=N_DEFAULT)
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--profile", action="store_true", help="plain W+K steps of --precision (for ncu)")
+    ap.add_argument("--calibrate-g", action="store_true", help="print the g of the self-interaction config")
     ap.add_argument("--precision", choices=["fp32", "fp64", "mixed"], default="mixed")
     ap.add_argument("--adjoint-steps", type=int, default=40, help="steps of the adjoint timing (0 skips it)")
     ap.add_argument("--g-phase", type=float, default=0.1,
@@ -618,6 +665,8 @@ def main():
         args.warmup = 3
     if args.profile:
         run_profile(args)
+    elif args.calibrate_g:
+        calibrate_g(args)
     elif args.impl == "reference":
         run_reference(args)
     else:

@@ -31,14 +31,21 @@ template <typename R, typename K, int N, int AXIS = 1> struct TmaTile {
     // lines per tile: 128-byte rows, except for the FP32 x passes at N = 512,
     // whose two chained transforms with compensated twiddles spill heavily at
     // the 64-register cap of 1024 threads; 8 lines (512 threads) do not spill
-    static constexpr int L = (SPLIT || (AXIS == 2 && sizeof(G) == 8 && N >= 512)) ? 8 : 128 / (int)sizeof(G);
+    static constexpr bool NARROW = !SPLIT && AXIS == 2 && sizeof(G) == 8 && N >= 512;
+    static constexpr int L = (SPLIT || NARROW) ? 8 : 128 / (int)sizeof(G);
     static constexpr int E = Plan<N>::E;
     static constexpr int T = N / E;
     static constexpr int NT = L * T;
     static constexpr int STAGES = 3;
     static constexpr int BOXR = N < 256 ? N : 256;               // rows per TMA box (limit 256)
     static constexpr size_t TILE_BYTES = size_t(N) * L * sizeof(G);
-    static constexpr size_t WORK_BYTES = SPLIT ? size_t(N) * L * sizeof(C) : 0;
+    // exchange tile between stages: the landing slot itself, or (mixed) a
+    // separate FP64 tile.  (A separate tile with rows padded to L + 1 for the
+    // narrow FP32 tiles, against their 2-way bank conflicts, measured slower:
+    // P3 0.94 -> 0.99 ms at 512^3.)
+    static constexpr bool OWN_WORK = SPLIT;
+    static constexpr int LPW = L;
+    static constexpr size_t WORK_BYTES = OWN_WORK ? size_t(N) * LPW * sizeof(C) : 0;
     static constexpr size_t SMEM = STAGES * TILE_BYTES + WORK_BYTES + 64;
     static_assert(NT <= 1024, "block size");
     static_assert(SMEM <= 227 * 1024, "shared memory per block");
@@ -101,12 +108,13 @@ __global__ void __launch_bounds__(TmaTile<R, K, N, AXIS>::NT, 1)
         constexpr int E = TL::E;
         C v[E];
         const G *land = bufs + (size_t)s * N * L;
-        C *wk = TL::SPLIT ? work : reinterpret_cast<C *>(bufs + (size_t)s * N * L);
+        C *wk = TL::OWN_WORK ? work : reinterpret_cast<C *>(bufs + (size_t)s * N * L);
+        constexpr int LPW = TL::LPW;
         // stage 0 straight from the landing slot
         stage_load<C, N, E, L, L, R0>(land, v, l, t);
-        if constexpr (TL::SPLIT) fence_proxy_async_smem();  // slot is released at the next barrier
+        if constexpr (TL::OWN_WORK) fence_proxy_async_smem();  // slot is released at the next barrier
         stage_compute<C, N, E, (MODE == 0 ? DIR : -1), R0, 1>(v, tw, t);
-        RegChain<C, N, E, (MODE == 0 ? DIR : -1), L, L, 1, R0>::run(wk, v, tw, l, t, true);
+        RegChain<C, N, E, (MODE == 0 ? DIR : -1), L, LPW, 1, R0>::run(wk, v, tw, l, t, true);
         if (MODE != 0) {
             // v[b*RL + r] holds element n = (t + T*b) + r*N/RL of the forward transform
             if (MODE == 1) {
@@ -139,7 +147,7 @@ __global__ void __launch_bounds__(TmaTile<R, K, N, AXIS>::NT, 1)
                         v[b * RL + r] = cscale(v[b * RL + r], k2 == 0 ? K(0) : K(-1) / K(k2));
                     }
             }
-            fft_regs_chained<C, N, E, +1, L, L>(wk, v, tw, l, t, true);
+            fft_regs_chained<C, N, E, +1, L, LPW>(wk, v, tw, l, t, true);
         }
         if ((g % W) < VW) {
             const size_t b0 = AXIS == 1 ? size_t(g / W) * N * W + size_t(g % W) : size_t(g);

@@ -130,7 +130,7 @@ __global__ void __launch_bounds__(TileZ<R, K, N>::NT)
         smr[2 * ((n >> 1) * TL::LP + l) + (n & 1)] = (K)src[row0 * N + f];
     }
     __syncthreads();
-    fft_tile<C, M, TL::EH, -1, TL::L, TL::LP>(sm, twh);
+    fft_tile<C, M, TL::EH, -1, TL::L, TL::LP, typename TL::HP>(sm, twh);
     for (int f = threadIdx.x; f < TL::L * NH; f += TL::NT) {
         const int l = f / NH, k = f % NH;
         const C zk = sm[(k % M) * TL::LP + l];

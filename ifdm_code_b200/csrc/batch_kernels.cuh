@@ -215,7 +215,7 @@ template <typename R, typename K, int N, class P> struct BatchOps {
             smr[2 * ((n >> 1) * TZ::LP + l) + (n & 1)] = rho[i];
         }
         __syncthreads();
-        fft_tile<C, M, TZ::EH, -1, TZ::L, TZ::LP>(sm, twh);
+        fft_tile<C, M, TZ::EH, -1, TZ::L, TZ::LP, typename TZ::HP>(sm, twh);
         for (int f = threadIdx.x; f < TZ::L * NH; f += TZ::NT) {
             const int l = f / NH, k = f % NH;
             const C zk = sm[(k % M) * TZ::LP + l];
@@ -284,7 +284,7 @@ template <typename R, typename K, int N, class P> struct BatchOps {
             sm[k * TZ::LP + l] = mkc(e.x - d.y, e.y + d.x);
         }
         __syncthreads();
-        fft_tile<C, M, TZ::EH, +1, TZ::L, TZ::LP>(sm, twh);
+        fft_tile<C, M, TZ::EH, +1, TZ::L, TZ::LP, typename TZ::HP>(sm, twh);
         const K *smr = reinterpret_cast<const K *>(sm);
         constexpr KSplit<K> inv(1.0 / ((double)N * N * N));
         double mx = 0.0;

@@ -223,14 +223,20 @@ struct StageLoop {
 
 // Elements per thread for a length-N line when T threads serve each line:
 // N / T when every radix divides it, else the plan's minimum.
-template <int N> __host__ __device__ constexpr bool divides_all(int e) {
-    for (int s = 0; s < Plan<N>::NST; ++s)
-        if (e % Plan<N>::R[s]) return false;
+template <int N, class P = Plan<N>> __host__ __device__ constexpr bool divides_all(int e) {
+    for (int s = 0; s < P::NST; ++s)
+        if (e % P::R[s]) return false;
     return true;
 }
-template <int N, int T> __host__ __device__ constexpr int elems_for(int) {
-    return (N % T == 0 && N / T >= Plan<N>::E && divides_all<N>(N / T)) ? N / T : Plan<N>::E;
+template <int N, int T, class P = Plan<N>> __host__ __device__ constexpr int elems_for(int) {
+    return (N % T == 0 && N / T >= P::E && divides_all<N, P>(N / T)) ? N / T : P::E;
 }
+
+// Plans of the half-length transforms of the real-to-complex passes: 256
+// points in radix 4 (4 elements per thread), so the 64 threads that serve a
+// 512-point line in the same block all take part (radix 8 would idle half).
+template <int M> struct HalfPlan : Plan<M> {};
+template <> struct HalfPlan<256> { static constexpr int E = 4, NST = 4; static constexpr int R[4] = {4, 4, 4, 4}; };
 
 // Transform all L lines of the tile in place, E elements per thread (threads
 // tid < L * (N / E) work; the rest only join the barriers).  Caller must

@@ -53,7 +53,8 @@ template <typename R, typename K, int N, bool ZR = false> struct Tile {
     static constexpr int E = E0;
     static constexpr int LP = L + 1;
     static constexpr int NT = L * T;                                // threads per block
-    static constexpr int EH = elems_for<N / 2, T>(0);               // half-length lines
+    using HP = HalfPlan<N / 2>;                                     // half-length lines
+    static constexpr int EH = elems_for<N / 2, T, HP>(0);
     static constexpr size_t SMEM = size_t(N) * LP * sizeof(C);
     static constexpr size_t SMEM9 = size_t(N + 1) * LP * sizeof(C);
     static_assert(N / E0 * E0 == N, "E must divide N");
@@ -299,7 +300,7 @@ __global__ void __launch_bounds__(TileZ<R, K, N>::NT)
         smr[2 * ((n >> 1) * TL::LP + l) + (n & 1)] = rho[i];
     }
     __syncthreads();
-    fft_tile<C, M, TL::EH, -1, TL::L, TL::LP>(sm, twh);
+    fft_tile<C, M, TL::EH, -1, TL::L, TL::LP, typename TL::HP>(sm, twh);
     // X_k = (Z_k + conj Z_{M-k})/2 - i w^k (Z_k - conj Z_{M-k})/2, k = 0..M
     for (int f = threadIdx.x; f < TL::L * NH; f += TL::NT) {
         const int l = f / NH, k = f % NH;
@@ -358,7 +359,7 @@ __global__ void __launch_bounds__(TileZ<R, K, N>::NT)
         sm[k * TL::LP + l] = mkc(e.x - d.y, e.y + d.x);
     }
     __syncthreads();
-    fft_tile<C, M, TL::EH, +1, TL::L, TL::LP>(sm, twh);
+    fft_tile<C, M, TL::EH, +1, TL::L, TL::LP, typename TL::HP>(sm, twh);
     const K *smr = reinterpret_cast<const K *>(sm);
     constexpr KSplit<K> inv(1.0 / ((double)N * N * N));
     double mx = 0.0;

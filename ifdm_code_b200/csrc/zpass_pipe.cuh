@@ -77,7 +77,7 @@ __global__ void __launch_bounds__(ZPipe<R, N>::NT, 1)
             smr[2 * ((n >> 1) * LP + l) + (n & 1)] = rho[e];
         }
         __syncthreads();
-        fft_tile<C, M, ZP::EH, -1, L, LP>(sm, twh);
+        fft_tile<C, M, ZP::EH, -1, L, LP, typename ZP::TL::HP>(sm, twh);
         for (int f = tid; f < L * NH; f += NT) {
             const int l = f / NH, k = f % NH;
             const C zk = sm[(k % M) * LP + l];

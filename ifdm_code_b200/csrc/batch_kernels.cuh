@@ -284,7 +284,7 @@ template <typename R, typename K, int N, class P> struct BatchOps {
             sm[k * TZ::LP + l] = mkc(e.x - d.y, e.y + d.x);
         }
         __syncthreads();
-        fft_tile<C, M, TZ::EH, +1, TZ::L, TZ::LP, typename TZ::HP>(sm, twh);
+        fft_tile<C, M, TZ::EHD, +1, TZ::L, TZ::LP>(sm, twh);
         const K *smr = reinterpret_cast<const K *>(sm);
         constexpr KSplit<K> inv(1.0 / ((double)N * N * N));
         double mx = 0.0;

@@ -28,6 +28,8 @@
 #pragma once
 
 #include "fft_engine.cuh"
+
+#include <type_traits>
 #include "state_types.hpp"
 
 namespace ifdm {
@@ -53,12 +55,16 @@ template <typename R, typename K, int N, bool ZR = false> struct Tile {
     static constexpr int E = E0;
     static constexpr int LP = L + 1;
     static constexpr int NT = L * T;                                // threads per block
-    using HP = HalfPlan<N / 2>;                                     // half-length lines
+    // half-length lines: the real-to-complex transform of P5 runs the radix-4
+    // plan in FP32 (measured at 512^3: P5 1.10 -> 1.02 ms; slower in FP64 and
+    // mixed, and for the complex-to-real P9), everything else the default plan
+    using HP = std::conditional_t<sizeof(C) == 8, HalfPlan<N / 2>, Plan<N / 2>>;
     static constexpr int EH = elems_for<N / 2, T, HP>(0);
+    static constexpr int EHD = elems_for<N / 2, T>(0);
     static constexpr size_t SMEM = size_t(N) * LP * sizeof(C);
     static constexpr size_t SMEM9 = size_t(N + 1) * LP * sizeof(C);
     static_assert(N / E0 * E0 == N, "E must divide N");
-    static_assert((N / 2) / EH <= T, "half-length lines must fit the block");
+    static_assert((N / 2) / EH <= T && (N / 2) / EHD <= T, "half-length lines must fit the block");
 };
 template <typename R, typename K, int N> using TileZ = Tile<R, K, N, true>;
 
@@ -359,7 +365,7 @@ __global__ void __launch_bounds__(TileZ<R, K, N>::NT)
         sm[k * TL::LP + l] = mkc(e.x - d.y, e.y + d.x);
     }
     __syncthreads();
-    fft_tile<C, M, TL::EH, +1, TL::L, TL::LP, typename TL::HP>(sm, twh);
+    fft_tile<C, M, TL::EHD, +1, TL::L, TL::LP>(sm, twh);
     const K *smr = reinterpret_cast<const K *>(sm);
     constexpr KSplit<K> inv(1.0 / ((double)N * N * N));
     double mx = 0.0;

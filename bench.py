@@ -270,7 +270,8 @@ def cpu_baseline_port(N: int, psi0, dt_scale: float):
 PROFILED_KERNEL = {("fp32", "P1"): "k_kick_fft_z<float,float,512>",
                    ("fp32", "P2"): "k_yx_tma<float,float,512,1,0,(int)-1>",
                    ("fp32", "P3"): "k_yx_tma<float,float,512,2,1,0>",
-                   ("fp32", "P5"): "k_density_r2c_z_pipe<float,512>"}
+                   ("fp32", "P5"): "k_density_r2c_z_pipe<float,512>",
+                   ("fp32", "P9"): "k_c2r_z_phi<float,float,512>"}
 
 
 def profiled_traffic(prec: str, pass_name: str, N: int):

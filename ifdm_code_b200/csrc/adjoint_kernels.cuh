@@ -131,8 +131,10 @@ __global__ void __launch_bounds__(TileZ<R, K, N>::NT)
     }
     __syncthreads();
     fft_tile<C, M, TL::EH, -1, TL::L, TL::LP, typename TL::HP>(sm, twh);
-    for (int f = threadIdx.x; f < TL::L * NH; f += TL::NT) {
-        const int l = f / NH, k = f % NH;
+    constexpr int TPR = TL::NT / TL::L;  // threads per row: no division by N/2+1
+    static_assert(TPR * TL::L == TL::NT, "whole rows per thread block");
+    const int l = threadIdx.x / TPR;
+    for (int k = threadIdx.x % TPR; k < NH; k += TPR) {
         const C zk = sm[(k % M) * TL::LP + l];
         const C zc = cconj(sm[((M - k) % M) * TL::LP + l]);
         const C e = cscale(zk + zc, K(0.5));

@@ -216,8 +216,10 @@ template <typename R, typename K, int N, class P> struct BatchOps {
         }
         __syncthreads();
         fft_tile<C, M, TZ::EH, -1, TZ::L, TZ::LP, typename TZ::HP>(sm, twh);
-        for (int f = threadIdx.x; f < TZ::L * NH; f += TZ::NT) {
-            const int l = f / NH, k = f % NH;
+        constexpr int TPR = TZ::NT / TZ::L;  // threads per row: no division by N/2+1
+        static_assert(TPR * TZ::L == TZ::NT, "whole rows per thread block");
+        const int l = threadIdx.x / TPR;
+        for (int k = threadIdx.x % TPR; k < NH; k += TPR) {
             const C zk = sm[(k % M) * TZ::LP + l];
             const C zc = cconj(sm[((M - k) % M) * TZ::LP + l]);
             const C e = cscale(zk + zc, K(0.5));
@@ -268,11 +270,14 @@ template <typename R, typename K, int N, class P> struct BatchOps {
         C *xs = sm + M * TZ::LP;
         const size_t row0 = size_t(tile) * TZ::L;
         const uint32_t salt = pass_salt(ts, 9);
-        for (int f = threadIdx.x; f < TZ::L * (M + 1); f += TZ::NT) {
-            const int l = f / (M + 1), k = f % (M + 1);
-            C x = cin<K>(rhok[(row0 + l) * NHP + k]);
-            if (k == 0 || k == M) x.y = K(0);
-            xs[k * TZ::LP + l] = x;
+        {
+            constexpr int TPR = TZ::NT / TZ::L;  // threads per row
+            const int l = threadIdx.x / TPR;
+            for (int k = threadIdx.x % TPR; k <= M; k += TPR) {
+                C x = cin<K>(rhok[(row0 + l) * NHP + k]);
+                if (k == 0 || k == M) x.y = K(0);
+                xs[k * TZ::LP + l] = x;
+            }
         }
         __syncthreads();
         for (int f = threadIdx.x; f < TZ::L * M; f += TZ::NT) {

@@ -308,8 +308,10 @@ __global__ void __launch_bounds__(TileZ<R, K, N>::NT)
     __syncthreads();
     fft_tile<C, M, TL::EH, -1, TL::L, TL::LP, typename TL::HP>(sm, twh);
     // X_k = (Z_k + conj Z_{M-k})/2 - i w^k (Z_k - conj Z_{M-k})/2, k = 0..M
-    for (int f = threadIdx.x; f < TL::L * NH; f += TL::NT) {
-        const int l = f / NH, k = f % NH;
+    constexpr int TPR = TL::NT / TL::L;  // threads per row: no division by N/2+1
+    static_assert(TPR * TL::L == TL::NT, "whole rows per thread block");
+    const int l = threadIdx.x / TPR;
+    for (int k = threadIdx.x % TPR; k < NH; k += TPR) {
         const C zk = sm[(k % M) * TL::LP + l];
         const C zc = cconj(sm[((M - k) % M) * TL::LP + l]);
         const C e = cscale(zk + zc, K(0.5));
@@ -336,19 +338,20 @@ __global__ void __launch_bounds__(TileZ<R, K, N>::NT)
     C *xs = sm + M * TL::LP;  // X_k rows k = 0..M staged after the Z tile
     const size_t row0 = size_t(blockIdx.x) * TL::L;
     const uint32_t salt = pass_salt(ts, 9);
-    // all of this thread's loads first, then the shared-memory stores
-    constexpr int PER = (TL::L * (M + 1) + TL::NT - 1) / TL::NT;
+    // all of this thread's loads first, then the shared-memory stores; TPR
+    // threads per row, so no division by N/2+1
+    constexpr int TPR = TL::NT / TL::L;
+    static_assert(TPR * TL::L == TL::NT, "whole rows per thread block");
+    constexpr int PER = (M + 1 + TPR - 1) / TPR;
+    const int l = threadIdx.x / TPR, k0 = threadIdx.x % TPR;
     typename TL::G g[PER];
 #pragma unroll
-    for (int i = 0; i < PER; ++i) {
-        const int f = threadIdx.x + i * TL::NT;
-        if (f < TL::L * (M + 1)) g[i] = rhok[(row0 + f / (M + 1)) * NHP + f % (M + 1)];
-    }
+    for (int i = 0; i < PER; ++i)
+        if (k0 + i * TPR <= M) g[i] = rhok[(row0 + l) * NHP + k0 + i * TPR];
 #pragma unroll
     for (int i = 0; i < PER; ++i) {
-        const int f = threadIdx.x + i * TL::NT;
-        if (f < TL::L * (M + 1)) {
-            const int l = f / (M + 1), k = f % (M + 1);
+        const int k = k0 + i * TPR;
+        if (k <= M) {
             C x = cin<K>(g[i]);
             if (k == 0 || k == M) x.y = K(0);  // c2r ignores these imaginary parts
             xs[k * TL::LP + l] = x;

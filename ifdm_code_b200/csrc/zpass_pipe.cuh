@@ -78,8 +78,10 @@ __global__ void __launch_bounds__(ZPipe<R, N>::NT, 1)
         }
         __syncthreads();
         fft_tile<C, M, ZP::EH, -1, L, LP, typename ZP::TL::HP>(sm, twh);
-        for (int f = tid; f < L * NH; f += NT) {
-            const int l = f / NH, k = f % NH;
+        constexpr int TPR = NT / L;  // threads per row: no division by N/2+1
+        static_assert(TPR * L == NT, "whole rows per thread block");
+        const int l = tid / TPR;
+        for (int k = tid % TPR; k < NH; k += TPR) {
             const C zk = sm[(k % M) * LP + l];
             const C zc = cconj(sm[((M - k) % M) * LP + l]);
             const C e = cscale(zk + zc, R(0.5));

@@ -288,6 +288,145 @@ def profiled_traffic(prec: str, pass_name: str, N: int):
     return None
 
 
+def snapshot_section(ifdm, N, prec, psi0, G, C, device, iters):
+    """Snapshots while stepping, two schedules: one after every step (the
+    reference's production state machine writes output<n>.dat each step
+    between a = 0.25 and 0.5, src/CosmoBEC_MPI_stan.cpp) and one every 50
+    steps.  Wall time per interval (steps + snapshot), three ways: steps
+    only; blocking (gather, copy and write inside the call, as the
+    reference's writeall); streamed (staged on the device, copied on a copy
+    stream and written by the writer thread beside the next steps).  Every
+    snapshot gets a new file name, as in the reference's runs (overwriting
+    a 2 GiB file costs its truncation, 0.7 s on the box's disk); the files are
+    deleted, and dirty pages synced, outside the timed regions."""
+    import shutil
+    import tempfile
+
+    fbytes = 16 * N ** 3 + 8 * (N + 3)
+    d = tempfile.mkdtemp(prefix="ifdm_snap_")
+    try:
+        free = shutil.disk_usage(d).free
+        if free < (iters + 3) * fbytes:
+            return {"skipped": f"{free / 1e9:.1f} GB free in {tempfile.gettempdir()}, "
+                               f"need {(iters + 3) * fbytes / 1e9:.1f}"}
+        out = {"res": N, "path": prec, "iterations": iters, "file_bytes": fbytes, "schedules": {}}
+        for every in (1, 50):
+            ms = {}
+            for mode in ("steps_only", "blocking", "streamed"):
+                sim = ifdm.Simulation(MFDM, G, XMAX, N, precision=prec, device=device, opath=d + "/")
+                sim.set_psi(psi0, A0)
+                sim.step(2, C)
+                sim.set_snapshot_streaming(mode == "streamed")
+                if mode != "steps_only":  # first use allocates the staging and pinned buffers
+                    sim.write_snapshot(9)
+                sim.synchronize()
+                os.sync()
+                t0 = time.perf_counter()
+                for i in range(iters):
+                    sim.step(every, C)
+                    if mode == "blocking":
+                        sim.write_snapshot(10 + i)
+                    elif mode == "streamed":
+                        sim.write_snapshot_async(10 + i)
+                sim.flush_snapshots()
+                sim.synchronize()
+                ms[mode] = (time.perf_counter() - t0) / iters * 1e3
+                sim.close()
+                for f in os.listdir(d):
+                    os.remove(os.path.join(d, f))
+            out["schedules"][f"every_{every}_steps"] = {
+                "ms_per_interval": {k: round(v, 3) for k, v in ms.items()},
+                "snapshot_cost_ms": {k: round(ms[k] - ms["steps_only"], 3) for k in ("blocking", "streamed")},
+                "blocking_over_streamed": round(ms["blocking"] / ms["streamed"], 3)}
+        out["note"] = ("wall clock around iters x (steps + snapshot), the last file flushed inside the timed "
+                       "region; buffered writes to the box's scratch disk")
+        return out
+    finally:
+        shutil.rmtree(d, ignore_errors=True)
+
+
+def ic_section(ifdm, N, device, cpu_res):
+    """Gadget IC pre-processing (src/gadget_IC.h:259-672) at N^3 particles:
+    four chunk files written to a scratch folder, then ifdm_load_ic timed
+    (files read side by side and streamed to the device, device CIC by a
+    stable radix sort by cell, divergence, spectral phase, psi), first call
+    and a repeat.  Size-independent check: the deposited mass equals the
+    particles' mass (ghost copies and the zero particle of each chunk
+    included, as one reference rank deposits them).  The oracle's IC on the
+    host cores at cpu_res^3 particles, per particle, stands beside it."""
+    import shutil
+    import tempfile
+
+    import numpy as np
+    import torch
+
+    from ifdm_code_b200.synthetic_ic import write_gadget_chunks, zeldovich_particles_device
+
+    d = tempfile.mkdtemp(prefix="ifdm_ic_")
+    try:
+        need = 28 * N ** 3 * 1.1
+        if shutil.disk_usage(d).free < need:
+            return {"skipped": f"{shutil.disk_usage(d).free / 1e9:.1f} GB free, need {need / 1e9:.1f}"}
+        t0 = time.perf_counter()
+        pos, vel, mass, a, box = zeldovich_particles_device(N, xmax=XMAX, seed=7, device=device)
+        torch.cuda.empty_cache()
+        write_gadget_chunks(d + "/ic", pos, vel, mass, a, box)
+        t_make = time.perf_counter() - t0
+        # slots one reference rank deposits: per chunk its particles, the
+        # trailing ones beyond the last cell centre again, and one zero particle
+        m = N ** 3 // 4
+        xg_last = (N - 1) * (box / N) + 0.5 * (box / N)
+        slots = 0
+        for c in range(4):
+            x = pos[c * m:(c + 1) * m, 0].astype(np.float64)
+            beyond = x[1:][::-1] > xg_last
+            lg = int(np.argmin(beyond)) if not beyond.all() else beyond.size
+            slots += m + lg + 1
+        del pos, vel
+        times = []
+        rho_sum = None
+        for rep in range(2):
+            with ifdm.Simulation(MFDM, 0.0, XMAX, N, opath=d + "/", icpath=d + "/ic", device=device) as sim:
+                sim.synchronize()
+                t0 = time.perf_counter()
+                sim.load_ic()
+                sim.synchronize()
+                times.append(time.perf_counter() - t0)
+                if rep == 1:
+                    psi = torch.empty((N, N, N), dtype=torch.complex128, device=f"cuda:{device}")
+                    sim.get_psi_into(psi)
+                    rho_sum = float((psi.real ** 2 + psi.imag ** 2).sum())
+                    del psi
+        # |psi|^2 = 1.225^2 rho h^2 1e9 / m_solar, rho = mass per cell / Lg^3 (Msun h^-1 / (kpc/h)^3)
+        consts = {"kg2eV": 1.783e-36, "kg2solar": 1.989e30, "h": 0.677}
+        m_solar = MFDM * consts["kg2eV"] / consts["kg2solar"]
+        Lg = box / N
+        want = 1.225 ** 2 * slots * mass * 1e10 / Lg ** 3 * consts["h"] ** 2 * 1e9 / m_solar
+        out = {"res": N, "particles": 4 * m, "particle_slots": slots, "files_gb": 28 * N ** 3 / 1e9,
+               "make_files_s": round(t_make, 2), "load_ic_s": round(times[0], 3), "load_ic_repeat_s": round(times[1], 3),
+               "particles_per_s": 4 * m / times[1],
+               "mass_rel_err": abs(rho_sum / want - 1.0)}
+    finally:
+        shutil.rmtree(d, ignore_errors=True)
+    if cpu_res:
+        from oracle import Oracle, OracleArgs
+        from ifdm_code_b200.synthetic_ic import make_ic
+
+        d = tempfile.mkdtemp(prefix="ifdm_ic_cpu_")
+        try:
+            make_ic(d + "/ic", cpu_res, seed=7)
+            o = Oracle(OracleArgs(res=cpu_res, mfdm=MFDM, xmax=XMAX, opath=d + "/", icpath=d + "/ic"))
+            t0 = time.perf_counter()
+            o.load_ic()
+            dt = time.perf_counter() - t0
+            o.close()
+            out["cpu_baseline"] = {"value": cpu_res ** 3 / dt, "unit": "particles/s", "cores": Oracle.num_threads(),
+                                   "kind": "port", "sample": f"oracle IC at {cpu_res}^3 particles ({dt:.1f} s)"}
+        finally:
+            shutil.rmtree(d, ignore_errors=True)
+    return out
+
+
 def run_ours(args):
     import numpy as np
     import torch
@@ -418,6 +557,12 @@ def run_ours(args):
 
     batch = {p: run_batch(args, p, local) for p in dict.fromkeys([head, "mixed"])} if args.batch_steps > 0 else None
 
+    ic = ic_section(ifdm, args.ic_res, local, 128 if not args.no_cpu_baseline else 0) if (
+        args.ic_res > 0 and rank == 0) else None
+
+    snaps = snapshot_section(ifdm, N, head, psi0, G, C, local, args.snapshot_steps) if (
+        args.snapshot_steps > 0 and rank == 0) else None
+
     # end to end through the C ABI with host buffers (pinned)
     pin_in = torch.from_numpy(psi0.view(np.float64)).pin_memory()
     pin_out = torch.empty_like(pin_in).pin_memory()
@@ -482,6 +627,8 @@ def run_ours(args):
         "cufft_reference": fft_ref,
         "adjoint": adj,
         "batch": batch,
+        "snapshots": snaps,
+        "ic": ic,
         "roofline": roofline(res[head], head),
         "e2e": {"value": e2e_value, "unit": "cell-steps/s", "h2d_bytes_per_step": 16 * cells / K,
                 "d2h_bytes_per_step": 16 * cells / K,
@@ -660,6 +807,10 @@ def main():
                          "reference's and this one) turns unstable above ~0.02 (max|psi|^2 x100 within 150 "
                          "steps at 0.1), so the benchmark uses 0.01")
     ap.add_argument("--batch-steps", type=int, default=500, help="steps of the 96-box batch timing (0 skips it)")
+    ap.add_argument("--ic-res", type=int, default=512,
+                    help="particles per side of the IC pre-processing timing (0 skips it)")
+    ap.add_argument("--snapshot-steps", type=int, default=4,
+                    help="snapshots per schedule of the blocking vs streamed timing (0 skips it)")
     ap.add_argument("--precision-steps", type=int, default=1000,
                     help="steps of the precision gate (density error vs FP64); 0 skips it")
     ap.add_argument("--ref-max-steps", type=int, default=3,

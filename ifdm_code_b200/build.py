@@ -1,9 +1,9 @@
-"""Build recipe for libifdm_b200.so and the BECMPI drop-in executable (sm_100a).
+"""Build recipe for libifdm_b200.so, the BECMPI drop-in executable and the readsnap tool (sm_100a).
 
     python -m ifdm_code_b200.build [--force] [--verbose]
 
 Objects go to ifdm_code_b200/_build/, the library to ifdm_code_b200/, the
-executable to ifdm_code_b200/bin/.  nvcc cross-compiles for sm_100a, so this
+executables to ifdm_code_b200/bin/.  nvcc cross-compiles for sm_100a, so this
 runs on machines without a GPU.
 """
 
@@ -22,6 +22,7 @@ INC = os.path.join(ROOT, "include")
 OBJ = os.path.join(PKG, "_build")
 LIB = os.path.join(PKG, "libifdm_b200.so")
 BIN = os.path.join(PKG, "bin", "BECMPI")
+READSNAP = os.path.join(PKG, "bin", "readsnap")
 
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 NVCC_FLAGS = ARCH + ["-O3", "-lineinfo", "-std=c++17", "-Xcompiler", "-fPIC", "--expt-relaxed-constexpr",
@@ -31,8 +32,8 @@ PER_FILE = {"ic_pipeline.cu": ["--fmad=false"]}
 CXX_FLAGS = ["-O2", "-fPIC", "-std=c++17", "-Wall", "-I" + CSRC, "-I" + INC]
 
 CU_SOURCES = ["step_engine.cu", "batch_engine.cu", "batch_fp64.cu", "batch_fp32.cu", "batch_mixed.cu",
-              "ic_pipeline.cu", "static_poisson.cu"]
-CPP_SOURCES = ["ifdm_api.cpp", "io.cpp"]
+              "ic_pipeline.cu", "static_poisson.cu", "diagnostics.cu"]
+CPP_SOURCES = ["ifdm_api.cpp", "io.cpp", "snapshot_stream.cpp", "ic_stream.cpp"]
 
 
 def _cuda_home() -> str:
@@ -102,7 +103,17 @@ def build(force: bool = False, verbose: bool = False) -> str:
     if force or _stale(BIN, main_src, hdr) or os.path.getmtime(BIN) < os.path.getmtime(LIB):
         _run(["g++", "-O2", "-std=c++17", "-I" + INC, main_src, "-o", BIN, "-L" + PKG, "-lifdm_b200",
               "-Wl,-rpath,$ORIGIN/.."], verbose)
+    build_readsnap(force, verbose)
     return LIB
+
+
+def build_readsnap(force: bool = False, verbose: bool = False) -> str:
+    """The host-only slice tool (no CUDA); returns its path."""
+    src = os.path.join(CSRC, "readsnap_main.cpp")
+    os.makedirs(os.path.dirname(READSNAP), exist_ok=True)
+    if force or _stale(READSNAP, src, os.path.getmtime(src)):
+        _run(["g++", "-O2", "-std=c++17", src, "-o", READSNAP], verbose)
+    return READSNAP
 
 
 if __name__ == "__main__":

@@ -3,11 +3,12 @@
 // sum below rounds exactly where the reference's does.
 //
 // CIC deposit as a deterministic sort-by-cell segmented reduction:
-//   1. each particle s (in the reference's processing order) emits one key
-//      (cell << 32 | s) per corner it deposits to (CIC_scheme,
-//      src/gadget_IC.h:45-156);
-//   2. keys are radix-sorted, so every cell's contributions sit together in
-//      particle order;
+//   1. each particle s (in the reference's processing order) emits one
+//      (cell, s) pair per corner it deposits to (CIC_scheme,
+//      src/gadget_IC.h:45-156), in s-major order;
+//   2. the pairs are radix-sorted by cell alone (32-bit keys, only the bits a
+//      cell index needs); the sort is stable, so every cell's contributions
+//      sit together in particle order;
 //   3. one thread per cell folds them in that order: density in FP64,
 //      velocities in FP32 with the reference's float += double rounding, so
 //      the result is bit-identical to the reference's sequential loop.
@@ -73,40 +74,44 @@ __device__ __forceinline__ bool cell_ok(const CicCell &c, int N) {
     return c.gi >= 0 && c.gi < N && c.gj >= 0 && c.gj < N && c.gk >= 0 && c.gk < N;
 }
 
-__global__ void k_cic_keys(const float *__restrict__ pos, long np, CicGeo g, unsigned long long *__restrict__ keys,
-                           int *__restrict__ bad) {
+// cells of the 8 corners of particle s at keys[8s..8s+7], s at vals[8s..8s+7]
+__global__ void k_cic_keys(const float *__restrict__ pos, long np, CicGeo g, unsigned *__restrict__ keys,
+                           unsigned *__restrict__ vals, int *__restrict__ bad) {
     const long s = long(blockIdx.x) * blockDim.x + threadIdx.x;
     if (s >= np) return;
     const CicCell c = cic_cell(g, pos[3 * s], pos[3 * s + 1], pos[3 * s + 2]);
-    unsigned long long *k = keys + 8 * s;
+    unsigned *k = keys + 8 * s, *v = vals + 8 * s;
+    const long N = g.N;
     if (!cell_ok(c, g.N)) {
         // outside [0, box): the reference indexes out of its arrays here; refuse
         atomicOr(bad, 1);
-        for (int q = 0; q < 8; ++q) k[q] = ~0ull;
+        for (int q = 0; q < 8; ++q) {
+            k[q] = unsigned(N * N * N);  // past every cell
+            v[q] = unsigned(s);
+        }
         return;
     }
-    const long N = g.N;
     const int ii[2] = {c.gi, c.gii}, jj[2] = {c.gj, c.gjj}, kk[2] = {c.gk, c.gkk};
     for (int q = 0; q < 8; ++q) {
-        const long cell = kk[q & 1] + N * (jj[(q >> 1) & 1] + N * ii[q >> 2]);
-        k[q] = ((unsigned long long)cell << 32) | (unsigned long long)s;
+        k[q] = unsigned(kk[q & 1] + N * (jj[(q >> 1) & 1] + N * ii[q >> 2]));
+        v[q] = unsigned(s);
     }
 }
 
-__global__ void k_cell_bounds(const unsigned long long *__restrict__ keys, long nk, long ncell, int *__restrict__ start,
+__global__ void k_cell_bounds(const unsigned *__restrict__ keys, long nk, long ncell, int *__restrict__ start,
                               int *__restrict__ end) {
     const long i = long(blockIdx.x) * blockDim.x + threadIdx.x;
     if (i >= nk) return;
-    const long c = (long)(keys[i] >> 32);
+    const long c = (long)keys[i];
     if (c >= ncell) return;
-    const long cp = i > 0 ? (long)(keys[i - 1] >> 32) : -1;
-    const long cn = i + 1 < nk ? (long)(keys[i + 1] >> 32) : -1;
+    const long cp = i > 0 ? (long)keys[i - 1] : -1;
+    const long cn = i + 1 < nk ? (long)keys[i + 1] : -1;
     if (c != cp) start[c] = (int)i;
     if (c != cn) end[c] = (int)(i + 1);
 }
 
 // one thread per cell: contributions in particle order
-__global__ void k_cic_fold(const unsigned long long *__restrict__ keys, const int *__restrict__ start,
+__global__ void k_cic_fold(const unsigned *__restrict__ vals, const int *__restrict__ start,
                            const int *__restrict__ end, const float *__restrict__ pos, const float *__restrict__ vel,
                            CicGeo g, double *__restrict__ rho, float *__restrict__ vx, float *__restrict__ vy,
                            float *__restrict__ vz) {
@@ -117,7 +122,7 @@ __global__ void k_cic_fold(const unsigned long long *__restrict__ keys, const in
     double r = 0.0;
     float ax = 0.f, ay = 0.f, az = 0.f;
     for (int i = start[cell]; i < end[cell]; ++i) {
-        const long s = (long)(keys[i] & 0xffffffffull);
+        const long s = (long)vals[i];
         const CicCell c = cic_cell(g, pos[3 * s], pos[3 * s + 1], pos[3 * s + 2]);
         const double X = (ci == c.gi) ? c.tx : c.dx;
         const double Y = (cj == c.gj) ? c.ty : c.dy;
@@ -192,12 +197,12 @@ __global__ void k_build_psi(const double *__restrict__ rho, const double2 *__res
 std::string ic_pipeline(const IcInput &in, double *d_psi_out, std::vector<float> *vx_out) {
     const int N = in.N;
     const long n3 = long(N) * N * N;
-    const long np = long(in.pos.size() / 3);
+    const long np = in.np;
     const long nk = 8 * np;
-    if (np >= (1L << 32) - 1) return "too many particles";
+    if (nk >= (1L << 31) - 1 || n3 >= (1L << 31)) return "too many particles or cells";
     CicGeo g{N, in.Lg, in.box, in.pmass, in.L3};
-    float *d_pos = nullptr, *d_vel = nullptr;
-    unsigned long long *d_keys = nullptr, *d_keys2 = nullptr;
+    const float *d_pos = in.d_pos, *d_vel = in.d_vel;
+    unsigned *d_keys = nullptr, *d_keys2 = nullptr, *d_vals = nullptr, *d_vals2 = nullptr;
     int *d_start = nullptr, *d_end = nullptr, *d_bad = nullptr;
     double *d_rho = nullptr;
     float *d_v = nullptr;
@@ -206,45 +211,45 @@ std::string ic_pipeline(const IcInput &in, double *d_psi_out, std::vector<float>
     size_t tmp_bytes = 0;
     std::string err;
     auto cleanup = [&]() {
-        cudaFree(d_pos); cudaFree(d_vel); cudaFree(d_keys); cudaFree(d_keys2); cudaFree(d_start);
+        cudaFree(d_keys); cudaFree(d_keys2); cudaFree(d_vals); cudaFree(d_vals2); cudaFree(d_start);
         cudaFree(d_end); cudaFree(d_bad); cudaFree(d_rho); cudaFree(d_v); cudaFree(d_th); cudaFree(d_tmp);
     };
     auto run = [&]() -> std::string {
         cudaStream_t s = in.stream;
-        CUDA_TRY(cudaMalloc(&d_pos, sizeof(float) * 3 * np));
-        CUDA_TRY(cudaMalloc(&d_vel, sizeof(float) * 3 * np));
-        CUDA_TRY(cudaMemcpyAsync(d_pos, in.pos.data(), sizeof(float) * 3 * np, cudaMemcpyHostToDevice, s));
-        CUDA_TRY(cudaMemcpyAsync(d_vel, in.vel.data(), sizeof(float) * 3 * np, cudaMemcpyHostToDevice, s));
-        CUDA_TRY(cudaMalloc(&d_keys, sizeof(unsigned long long) * nk));
-        CUDA_TRY(cudaMalloc(&d_keys2, sizeof(unsigned long long) * nk));
+        CUDA_TRY(cudaMalloc(&d_keys, sizeof(unsigned) * nk));
+        CUDA_TRY(cudaMalloc(&d_keys2, sizeof(unsigned) * nk));
+        CUDA_TRY(cudaMalloc(&d_vals, sizeof(unsigned) * nk));
+        CUDA_TRY(cudaMalloc(&d_vals2, sizeof(unsigned) * nk));
         CUDA_TRY(cudaMalloc(&d_bad, sizeof(int)));
         CUDA_TRY(cudaMemsetAsync(d_bad, 0, sizeof(int), s));
-        k_cic_keys<<<unsigned((np + 255) / 256), 256, 0, s>>>(d_pos, np, g, d_keys, d_bad);
+        k_cic_keys<<<unsigned((np + 255) / 256), 256, 0, s>>>(d_pos, np, g, d_keys, d_vals, d_bad);
         CUDA_TRY(cudaGetLastError());
-        int end_bit = 32;
-        while ((1L << (end_bit - 32)) < n3 + 1) ++end_bit;
-        CUDA_TRY(cub::DeviceRadixSort::SortKeys(nullptr, tmp_bytes, d_keys, d_keys2, nk, 0, end_bit + 1, s));
+        int end_bit = 1;  // keys 0..n3 (n3 marks a refused particle)
+        while ((1L << end_bit) <= n3) ++end_bit;
+        cub::DoubleBuffer<unsigned> kb(d_keys, d_keys2), vb(d_vals, d_vals2);
+        CUDA_TRY(cub::DeviceRadixSort::SortPairs(nullptr, tmp_bytes, kb, vb, (int)nk, 0, end_bit, s));
         CUDA_TRY(cudaMalloc(&d_tmp, tmp_bytes));
-        CUDA_TRY(cub::DeviceRadixSort::SortKeys(d_tmp, tmp_bytes, d_keys, d_keys2, nk, 0, end_bit + 1, s));
-        cudaFree(d_keys);
-        d_keys = nullptr;
+        CUDA_TRY(cub::DeviceRadixSort::SortPairs(d_tmp, tmp_bytes, kb, vb, (int)nk, 0, end_bit, s));
+        const unsigned *sk = kb.Current(), *sv = vb.Current();
         CUDA_TRY(cudaMalloc(&d_start, sizeof(int) * n3));
         CUDA_TRY(cudaMalloc(&d_end, sizeof(int) * n3));
         CUDA_TRY(cudaMemsetAsync(d_start, 0, sizeof(int) * n3, s));
         CUDA_TRY(cudaMemsetAsync(d_end, 0, sizeof(int) * n3, s));
-        k_cell_bounds<<<unsigned((nk + 255) / 256), 256, 0, s>>>(d_keys2, nk, n3, d_start, d_end);
+        k_cell_bounds<<<unsigned((nk + 255) / 256), 256, 0, s>>>(sk, nk, n3, d_start, d_end);
         CUDA_TRY(cudaGetLastError());
         CUDA_TRY(cudaMalloc(&d_rho, sizeof(double) * n3));
         CUDA_TRY(cudaMalloc(&d_v, sizeof(float) * 3 * n3));
         float *vx = d_v, *vy = d_v + n3, *vz = d_v + 2 * n3;
-        k_cic_fold<<<unsigned((n3 + 127) / 128), 128, 0, s>>>(d_keys2, d_start, d_end, d_pos, d_vel, g, d_rho, vx, vy,
-                                                              vz);
+        k_cic_fold<<<unsigned((n3 + 127) / 128), 128, 0, s>>>(sv, d_start, d_end, d_pos, d_vel, g, d_rho, vx, vy, vz);
         CUDA_TRY(cudaGetLastError());
         int bad = 0;
         CUDA_TRY(cudaMemcpyAsync(&bad, d_bad, sizeof(int), cudaMemcpyDeviceToHost, s));
         CUDA_TRY(cudaStreamSynchronize(s));
         if (bad) return "IC particle outside [0, BoxSize)";
+        cudaFree(d_keys); d_keys = nullptr;
         cudaFree(d_keys2); d_keys2 = nullptr;
+        cudaFree(d_vals); d_vals = nullptr;
+        cudaFree(d_vals2); d_vals2 = nullptr;
         cudaFree(d_tmp); d_tmp = nullptr;
         // velocity phase
         CUDA_TRY(cudaMalloc(&d_th, sizeof(double2) * n3));

@@ -19,7 +19,8 @@ struct IcInput {
     double kf = 0;           // mfdm / pow(c,2) / hbar
     double uc_rho = 0;       // pow(h_0,2) * pow(1e3,3)
     double uc_vel = 0;       // 1e3 / m2Mpc * s2Myr
-    std::vector<float> pos, vel;  // particles in the reference's processing order
+    const float *d_pos = nullptr, *d_vel = nullptr;  // device, 3 floats per particle, in the
+    long np = 0;                                     // reference's processing order
     cudaStream_t stream = nullptr;
 };
 

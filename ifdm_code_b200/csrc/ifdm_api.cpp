@@ -12,9 +12,12 @@
 #include <vector>
 
 #include "batch_engine.hpp"
+#include "diagnostics.hpp"
 #include "ic_pipeline.hpp"
+#include "ic_stream.hpp"
 #include "io.hpp"
 #include "physics.hpp"
+#include "snapshot_stream.hpp"
 #include "step_engine.hpp"
 
 using namespace ifdm;
@@ -33,6 +36,8 @@ struct ifdm_ctx {
     double *d_out = nullptr;   // complex128 N^3 device staging for outputs
     double *h_out = nullptr;   // pinned host staging
     size_t h_out_bytes = 0;
+    bool stream_snapshots = true;  // snapshots copied and written beside the steps
+    SnapshotStream snap;
 };
 
 static int fail(ifdm_ctx *c, int code, const std::string &msg) {
@@ -129,6 +134,7 @@ int ifdm_create(const ifdm_params *p, ifdm_ctx **out) {
 
 void ifdm_destroy(ifdm_ctx *c) {
     if (!c) return;
+    c->snap.drain();
     if (c->stream) cudaStreamSynchronize(c->stream);
     cudaFree(c->d_out);
     if (c->h_out) cudaFreeHost(c->h_out);
@@ -179,6 +185,7 @@ static int psi_to_host(ifdm_ctx *c, double *host, int which) {
         return IFDM_OK;
     }
     if (ensure_out(c)) return IFDM_ERR_CUDA;
+    if (c->snap.ready()) CTX_STR(c, IFDM_ERR_CUDA, c->snap.before_stage(c->stream));
     CTX_STR(c, IFDM_ERR_CUDA, c->eng.psi_out(c->d_out, which));
     CTX_CUDA(c, cudaMemcpyAsync(host, c->d_out, c->eng.n3() * 2 * sizeof(double), cudaMemcpyDeviceToHost, c->stream));
     CTX_CUDA(c, cudaStreamSynchronize(c->stream));
@@ -195,9 +202,22 @@ int ifdm_get_phi(ifdm_ctx *c, double *phi) {
     if (!c || !phi) return IFDM_ERR_ARGS;
     if (!c->have_psi) return fail(c, IFDM_ERR_STATE, "no wave function loaded");
     if (ensure_out(c)) return IFDM_ERR_CUDA;
+    if (c->snap.ready()) CTX_STR(c, IFDM_ERR_CUDA, c->snap.before_stage(c->stream));
     CTX_STR(c, IFDM_ERR_CUDA, c->eng.phi_out(c->d_out));
     CTX_CUDA(c, cudaMemcpyAsync(phi, c->d_out, c->eng.n3() * sizeof(double), cudaMemcpyDeviceToHost, c->stream));
     CTX_CUDA(c, cudaStreamSynchronize(c->stream));
+    return IFDM_OK;
+}
+
+int ifdm_power_spectrum(ifdm_ctx *c, int nbins, const double *edges, double *k, double *pk, long long *modes,
+                        double *mean_rho) {
+    if (!c || nbins < 1 || nbins > kMaxBins) return fail(c, IFDM_ERR_ARGS, "nbins must be 1..64");
+    if (!c->have_psi) return fail(c, IFDM_ERR_STATE, "no wave function loaded");
+    if (ensure_out(c)) return IFDM_ERR_CUDA;
+    if (c->snap.ready()) CTX_STR(c, IFDM_ERR_CUDA, c->snap.before_stage(c->stream));
+    CTX_STR(c, IFDM_ERR_CUDA, c->eng.psi_out(c->d_out, 2));
+    CTX_STR(c, IFDM_ERR_ARGS, power_spectrum(reinterpret_cast<double2 *>(c->d_out), c->N, 2.0 * c->xmax, nbins, edges,
+                                             k, pk, modes, mean_rho, c->stream));
     return IFDM_OK;
 }
 
@@ -221,6 +241,17 @@ int ifdm_get_state(ifdm_ctx *c, ifdm_state *out) {
 static int write_snapshot_which(ifdm_ctx *c, int t, int which, double a) {
     const size_t n3 = c->eng.n3();
     const size_t bytes = n3 * 2 * sizeof(double);
+    const double gg = c->g * (pow(phys::cm2Mpc, 3));
+    if (c->stream_snapshots) {
+        // psi into the device staging buffer on the compute stream; the copy
+        // to the host and the file write go on beside the next steps
+        if (ensure_out(c)) return IFDM_ERR_CUDA;
+        CTX_STR(c, IFDM_ERR_CUDA, c->snap.init(bytes, c->p.device));
+        CTX_STR(c, IFDM_ERR_CUDA, c->snap.before_stage(c->stream));
+        CTX_STR(c, IFDM_ERR_CUDA, c->eng.psi_out(c->d_out, which));
+        CTX_STR(c, IFDM_ERR_IO, c->snap.submit(c->stream, c->d_out, snapshot_path(c->opath, t), c->mfdm, gg, a, c->x));
+        return IFDM_OK;
+    }
     if (c->h_out_bytes < bytes) {
         if (c->h_out) cudaFreeHost(c->h_out);
         c->h_out = nullptr;
@@ -230,18 +261,38 @@ static int write_snapshot_which(ifdm_ctx *c, int t, int which, double a) {
     }
     int rc = psi_to_host(c, c->h_out, which);
     if (rc) return rc;
-    const double gg = c->g * (pow(phys::cm2Mpc, 3));
     CTX_STR(c, IFDM_ERR_IO, write_snapshot(snapshot_path(c->opath, t), c->mfdm, gg, a, c->x, c->h_out, n3));
     return IFDM_OK;
 }
 
-int ifdm_write_snapshot(ifdm_ctx *c, int t) {
+int ifdm_write_snapshot_async(ifdm_ctx *c, int t) {
     if (!c) return IFDM_ERR_ARGS;
     if (!c->have_psi) return fail(c, IFDM_ERR_STATE, "no wave function loaded");
     TState st{};
     CTX_STR(c, IFDM_ERR_CUDA, c->eng.read_state(st));
     return write_snapshot_which(c, t, 2, st.steps ? st.a : c->a0);
 }
+
+int ifdm_flush_snapshots(ifdm_ctx *c) {
+    if (!c) return IFDM_ERR_ARGS;
+    CTX_STR(c, IFDM_ERR_IO, c->snap.drain());
+    return IFDM_OK;
+}
+
+int ifdm_write_snapshot(ifdm_ctx *c, int t) {
+    const int rc = ifdm_write_snapshot_async(c, t);
+    return rc ? rc : ifdm_flush_snapshots(c);
+}
+
+int ifdm_set_snapshot_streaming(ifdm_ctx *c, int on) {
+    if (!c) return IFDM_ERR_ARGS;
+    const int rc = ifdm_flush_snapshots(c);
+    if (rc) return rc;
+    c->stream_snapshots = on != 0;
+    return IFDM_OK;
+}
+
+long long ifdm_snapshots_written(const ifdm_ctx *c) { return c ? c->snap.written() : -1; }
 
 int ifdm_load_snapshot(ifdm_ctx *c, int t) {
     if (!c) return IFDM_ERR_ARGS;
@@ -258,18 +309,21 @@ int ifdm_load_ic(ifdm_ctx *c) {
     if (!c) return IFDM_ERR_ARGS;
     using namespace phys;
     const int N = c->N;
-    IcInput in;
-    in.N = N;
+    const int tot_chunks = 4;  // src/gadget_IC.h:610
+    const bool ref1 = c->p.ic_mode == IFDM_IC_REF1;
+    std::vector<IcChunk> chunks;
+    long np = 0;
+    // headers (and ghost counts) of all chunks; a read problem in chunk k is
+    // reported after chunks 0..k-1 passed their checks, as the reference's
+    // chunk-by-chunk loop would
+    const std::string scan_err = ic_scan_chunks(c->icpath, tot_chunks, N, ref1, &chunks, &np);
     GadgetHeader hd{};
     double rhoc = 0, a = 0;
-    const int tot_chunks = 4;  // src/gadget_IC.h:610
-    for (int chunk = 0; chunk < tot_chunks; ++chunk) {
-        std::vector<float> pos, vel;
-        CTX_STR(c, IFDM_ERR_IO, read_gadget_chunk(c->icpath + "." + std::to_string(chunk), &hd, &pos, &vel));
+    for (const IcChunk &ch : chunks) {
+        hd = ch.h;
         if (c->p.verbose)
-            std::printf("read file from %s.%d\nnpart = %d\nmass = %g\na = %g\nredshift? = %g\nBoxSize = %g\nh = %g \n",
-                        c->icpath.c_str(), chunk, hd.npart[1], hd.mass[1], hd.time, hd.redshift, hd.BoxSize,
-                        hd.HubbleParam);
+            std::printf("read file from %s\nnpart = %d\nmass = %g\na = %g\nredshift? = %g\nBoxSize = %g\nh = %g \n",
+                        ch.path.c_str(), hd.npart[1], hd.mass[1], hd.time, hd.redshift, hd.BoxSize, hd.HubbleParam);
         // src/gadget_IC.h:309-314
         if (!(std::fabs(hd.BoxSize - 2 * c->xmax * 1e3 * h_0) < 0.001)) {
             char msg[256];
@@ -280,34 +334,12 @@ int ifdm_load_ic(ifdm_ctx *c) {
         hd.mass[1] *= 1e10;
         a = hd.time;
         rhoc = tot_chunks * hd.npart[1] * hd.mass[1] / pow(hd.BoxSize, 3) * pow(1e3, 3) * pow(h_0, 2);
-        const double Lg = hd.BoxSize / N;
-        const long n = hd.npart[1];
-        if (c->p.ic_mode == IFDM_IC_REF1) {
-            // one rank: trailing particles beyond the last cell centre are rank
-            // 0's left ghosts and also its own (src/gadget_IC.h:445-448,
-            // :496-502), then numpart + 1 owned particles, the extra one zero
-            // (src/gadget_IC.h:431-432)
-            const double xg_last = (N - 1) * Lg + 0.5 * Lg;
-            long lg = 0;
-            for (long pn = n - 1; pn > 0; pn--) {
-                if (xg_last < pos[3 * pn]) lg++;
-                else break;
-            }
-            in.pos.insert(in.pos.end(), pos.end() - 3 * lg, pos.end());
-            in.vel.insert(in.vel.end(), vel.end() - 3 * lg, vel.end());
-            in.pos.insert(in.pos.end(), pos.begin(), pos.end());
-            in.vel.insert(in.vel.end(), vel.begin(), vel.end());
-            for (int q = 0; q < 3; ++q) {
-                in.pos.push_back(0.f);
-                in.vel.push_back(0.f);
-            }
-        } else {
-            in.pos.insert(in.pos.end(), pos.begin(), pos.end());
-            in.vel.insert(in.vel.end(), vel.begin(), vel.end());
-        }
-        in.Lg = Lg;
-        in.box = hd.BoxSize;
     }
+    if (!scan_err.empty()) return fail(c, IFDM_ERR_IO, scan_err);
+    IcInput in;
+    in.N = N;
+    in.Lg = hd.BoxSize / N;
+    in.box = hd.BoxSize;
     in.pmass = hd.mass[1];
     in.L3 = pow(in.Lg, 3);
     in.a = a;
@@ -318,9 +350,20 @@ int ifdm_load_ic(ifdm_ctx *c) {
     in.uc_rho = pow(h_0, 2) * pow(1e3, 3);
     in.uc_vel = 1e3 / m2Mpc * s2Myr;
     in.stream = c->stream;
+    in.np = np;
     if (ensure_out(c)) return IFDM_ERR_CUDA;
+    // particles straight from the files into device memory (ic_stream.hpp)
+    float *d_part = nullptr;
+    CTX_CUDA(c, cudaMalloc(&d_part, sizeof(float) * 6 * size_t(np > 0 ? np : 1)));
+    std::string err = ic_upload(chunks, ref1, d_part, d_part + 3 * np, c->p.device);
     std::vector<float> vx;
-    CTX_STR(c, IFDM_ERR_CUDA, ic_pipeline(in, c->d_out, &vx));
+    if (err.empty()) {
+        in.d_pos = d_part;
+        in.d_vel = d_part + 3 * np;
+        err = ic_pipeline(in, c->d_out, &vx);
+    }
+    cudaFree(d_part);
+    if (!err.empty()) return fail(c, err.find("Gadget") != std::string::npos ? IFDM_ERR_IO : IFDM_ERR_CUDA, err);
     CTX_STR(c, IFDM_ERR_IO, write_voutput(c->opath + "voutput.dat", vx.data(), vx.size()));
     return ifdm_set_psi(c, c->d_out, a, rhoc);
 }
@@ -333,9 +376,18 @@ int ifdm_step(ifdm_ctx *c, int nsteps, double dt_scale) {
 }
 
 // Simulation (src/CosmoBEC_MPI.cpp:183-310)
+static int run_loop(ifdm_ctx *c);
 int ifdm_run(ifdm_ctx *c) {
     if (!c) return IFDM_ERR_ARGS;
     if (!c->have_psi) return fail(c, IFDM_ERR_STATE, "no wave function loaded");
+    int rc = run_loop(c);
+    // every snapshot file is complete when the run returns, as in the reference
+    const std::string e = c->snap.drain();
+    if (rc == IFDM_OK && !e.empty()) rc = fail(c, IFDM_ERR_IO, e);
+    return rc;
+}
+
+static int run_loop(ifdm_ctx *c) {
     const bool v = c->p.verbose != 0;
     int write_num = 0;
     int write_sten_counter = 2;

@@ -1,4 +1,4 @@
-// io.cpp -- snapshot, voutput and Gadget chunk I/O (formats in io.hpp).
+// io.cpp -- snapshot and voutput I/O (formats in io.hpp; Gadget chunks are read by ic_stream.cpp).
 #include "io.hpp"
 
 #include <cstdio>
@@ -49,32 +49,6 @@ std::string write_voutput(const std::string &path, const float *vx, size_t n3) {
     bool ok = std::fwrite(vx, sizeof(float), n3, f) == n3;
     ok = (std::fclose(f) == 0) && ok;
     return ok ? "" : "short write to " + path;
-}
-
-std::string read_gadget_chunk(const std::string &path, GadgetHeader *h, std::vector<float> *pos,
-                              std::vector<float> *vel) {
-    FILE *f = std::fopen(path.c_str(), "rb");
-    if (!f) return " cannot read IC file !! " + path;
-    int b0 = 0, b1 = 0;
-    bool ok = std::fread(&b0, 4, 1, f) == 1 && std::fread(h, sizeof(GadgetHeader), 1, f) == 1 &&
-              std::fread(&b1, 4, 1, f) == 1;
-    if (!ok) {
-        std::fclose(f);
-        return "truncated Gadget header " + path;
-    }
-    const long n = h->npart[1];
-    if (n < 0) {
-        std::fclose(f);
-        return "bad particle count in " + path;
-    }
-    pos->assign(size_t(3 * n), 0.f);
-    vel->assign(size_t(3 * n), 0.f);
-    int blk = 0;
-    ok = std::fread(&blk, 4, 1, f) == 1 && std::fread(pos->data(), sizeof(float), size_t(3 * n), f) == size_t(3 * n);
-    ok = ok && std::fread(&blk, 4, 1, f) == 1 && std::fread(&blk, 4, 1, f) == 1;
-    ok = ok && std::fread(vel->data(), sizeof(float), size_t(3 * n), f) == size_t(3 * n);
-    std::fclose(f);
-    return ok ? "" : "truncated Gadget blocks " + path;
 }
 
 }  // namespace ifdm

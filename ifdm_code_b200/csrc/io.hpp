@@ -43,8 +43,5 @@ std::string write_snapshot(const std::string &path, double mfdm, double g_cm3, d
 // Reads a, x and psi of an N^3 snapshot (psi may be null to read the header only).
 std::string read_snapshot(const std::string &path, int N, double *a, std::vector<double> *x, double *psi);
 std::string write_voutput(const std::string &path, const float *vx, size_t n3);
-// One Gadget chunk: header, positions and velocities (3*npart floats each).
-std::string read_gadget_chunk(const std::string &path, GadgetHeader *h, std::vector<float> *pos,
-                              std::vector<float> *vel);
 
 }  // namespace ifdm

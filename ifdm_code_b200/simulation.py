@@ -117,6 +117,25 @@ class Simulation:
         self._c(self.lib.ifdm_get_phi(self.h, out.ctypes.data_as(C.c_void_p)))
         return out
 
+    def power_spectrum(self, nbins: int = 24, edges=None) -> dict:
+        """P(k) of the density contrast of the current state, on the device.
+        edges: nbins+1 increasing |kappa| bin edges (integer wave-vector
+        units); None: log-spaced from 1 to N/2.  Returns k [1/Mpc], pk
+        [Mpc^3], modes per bin and <|psi|^2>."""
+        k = np.zeros(nbins)
+        pk = np.zeros(nbins)
+        modes = np.zeros(nbins, dtype=np.int64)
+        mean = C.c_double()
+        e = None
+        if edges is not None:
+            e = np.ascontiguousarray(edges, dtype=np.float64)
+            if e.shape != (nbins + 1,):
+                raise ValueError("edges needs nbins + 1 values")
+        self._c(self.lib.ifdm_power_spectrum(self.h, nbins, None if e is None else e.ctypes.data_as(C.c_void_p),
+                                             k.ctypes.data_as(C.c_void_p), pk.ctypes.data_as(C.c_void_p),
+                                             modes.ctypes.data_as(C.c_void_p), C.byref(mean)))
+        return {"k": k, "pk": pk, "modes": modes, "mean_rho": mean.value}
+
     def state(self) -> dict:
         s = State()
         self._c(self.lib.ifdm_get_state(self.h, C.byref(s)))
@@ -130,7 +149,25 @@ class Simulation:
         self._c(self.lib.ifdm_step(self.h, nsteps, dt_scale))
 
     def write_snapshot(self, t: int) -> None:
+        """<opath>output<t>.dat of the current state, complete on return."""
         self._c(self.lib.ifdm_write_snapshot(self.h, t))
+
+    def write_snapshot_async(self, t: int) -> None:
+        """Queue <opath>output<t>.dat; it is written while later steps run."""
+        self._c(self.lib.ifdm_write_snapshot_async(self.h, t))
+
+    def flush_snapshots(self) -> None:
+        """Wait until every queued snapshot file is written."""
+        self._c(self.lib.ifdm_flush_snapshots(self.h))
+
+    def set_snapshot_streaming(self, on: bool) -> None:
+        """False: gather and write each snapshot inside the call (the
+        reference's blocking writeall)."""
+        self._c(self.lib.ifdm_set_snapshot_streaming(self.h, 1 if on else 0))
+
+    @property
+    def snapshots_written(self) -> int:
+        return int(self.lib.ifdm_snapshots_written(self.h))
 
     def synchronize(self) -> None:
         self._c(self.lib.ifdm_synchronize(self.h))

@@ -113,6 +113,17 @@ int ifdm_get_psi(ifdm_ctx *ctx, double *psi);
 /* phi (N^3 doubles) of the current density. */
 int ifdm_get_phi(ifdm_ctx *ctx, double *phi);
 int ifdm_get_state(ifdm_ctx *ctx, ifdm_state *out);
+/* Power spectrum of the density contrast delta = |psi|^2/<|psi|^2> - 1 of the
+ * current state, computed on the device (an extension: the reference has no
+ * such output).  Bin b holds the modes with edges[b] <= |kappa| < edges[b+1],
+ * kappa the integer wave vector (-N/2..N/2-1 per axis); edges = NULL gives
+ * nbins log-spaced bins from 1 to N/2.  Outputs (each may be NULL; nbins
+ * entries): k = mean 2 pi |kappa| / L of the bin's modes [1/Mpc], pk =
+ * <|delta_k|^2> L^3 / N^6 [Mpc^3] with delta_k the unnormalised forward DFT,
+ * modes = modes per bin; mean_rho = <|psi|^2>.  L = 2 xmax (Mpc).
+ * nbins <= 64.  Every sum has a fixed order: repeated calls agree bit for bit. */
+int ifdm_power_spectrum(ifdm_ctx *ctx, int nbins, const double *edges, double *k, double *pk, long long *modes,
+                        double *mean_rho);
 
 /* Simulation (src/CosmoBEC_MPI.cpp:183-310): steps ti..t_stop-1 with the
  * adaptive timestep, the snapshot state machine and its early stops. */
@@ -121,8 +132,24 @@ int ifdm_run(ifdm_ctx *ctx);
  * selected timestep multiplied by dt_scale (1.0 = the reference's rule).
  * Asynchronous on the context's stream. */
 int ifdm_step(ifdm_ctx *ctx, int nsteps, double dt_scale);
-/* writeall (src/write3D.h:86-97): <opath>output<t>.dat of the current state. */
+/* writeall (src/write3D.h:86-97): <opath>output<t>.dat of the current state;
+ * the file is complete on return. */
 int ifdm_write_snapshot(ifdm_ctx *ctx, int t);
+/* Snapshot streaming (an extension; the reference's writeall blocks the
+ * loop).  With streaming on (the default) a snapshot costs the compute stream
+ * one kernel into a device staging buffer; the copy to pinned host memory runs
+ * on a copy stream and a writer thread writes the file while the steps go on.
+ * The bytes are those of the synchronous path.  ifdm_run returns only after
+ * every file is written.
+ *   ifdm_write_snapshot_async  queue <opath>output<t>.dat and return
+ *   ifdm_flush_snapshots       wait for queued files; first write error
+ *   ifdm_set_snapshot_streaming  0: gather and write inside the call, as
+ *                              the reference does (flushes first)
+ *   ifdm_snapshots_written     files written by the streaming writer */
+int ifdm_write_snapshot_async(ifdm_ctx *ctx, int t);
+int ifdm_flush_snapshots(ifdm_ctx *ctx);
+int ifdm_set_snapshot_streaming(ifdm_ctx *ctx, int on);
+long long ifdm_snapshots_written(const ifdm_ctx *ctx);
 int ifdm_synchronize(ifdm_ctx *ctx);
 /* The context's cudaStream_t (as void*). */
 void *ifdm_stream(ifdm_ctx *ctx);

@@ -8,6 +8,9 @@ reference sources compiled unmodified against single-rank MPI/FFTW/GSL shims):
 Each case runs ``oracle/_ref/BECMPI_ref`` (or ``BECMPI_ref_stan``) with the
 reference's 10-argument command line on a seeded synthetic IC and keeps the
 snapshot files it writes.  ``manifest.json`` records the command lines.
+``readsnap/`` holds the text slices the reference's ``src/readsnap.cpp``
+(``oracle/_ref/readsnap_ref``) makes of some of those snapshots;
+``python tests/golden/make_golden.py readsnap`` regenerates only them.
 """
 
 from __future__ import annotations
@@ -78,14 +81,44 @@ def run_rerun():
             "files": sorted(f for f in os.listdir(out) if f.endswith(".dat"))}
 
 
+# readsnap cases: snapshot of ref16 (written by the reference), z slices
+READSNAP_CASES = [("ref16", 16, 11, 0), ("ref16", 16, 11, 5), ("ref16", 16, 999997, 15)]
+
+
+def run_readsnap():
+    """The reference's slice tool (oracle/_ref/readsnap_ref) on reference snapshots."""
+    tool = os.path.join(ROOT, "oracle", "_ref", "readsnap_ref")
+    out = os.path.join(HERE, "readsnap")
+    if os.path.exists(out):
+        shutil.rmtree(out)
+    os.makedirs(out)
+    cases = []
+    for src, N, t, z in READSNAP_CASES:
+        r = subprocess.run([tool, str(N), str(z), str(t), os.path.join(HERE, src), out], capture_output=True,
+                           text=True, check=True)
+        name = f"output{t}.dat.z{z}"
+        with open(os.path.join(out, name + ".stdout"), "w") as f:
+            f.write(r.stdout.replace(HERE + "/", "<golden>/"))
+        cases.append({"src": src, "N": N, "t": t, "z": z, "file": name})
+    return {"binary": "readsnap_ref", "cases": cases}
+
+
 def main():
     build()
     if ref_binary() is None:
         raise SystemExit("oracle/_ref/BECMPI_ref is not built (reference sources absent)")
+    if sys.argv[1:] == ["readsnap"]:
+        with open(os.path.join(HERE, "manifest.json")) as f:
+            manifest = json.load(f)
+        manifest["readsnap"] = run_readsnap()
+        with open(os.path.join(HERE, "manifest.json"), "w") as f:
+            json.dump(manifest, f, indent=1)
+        return
     manifest = {}
     for c in CASES:
         manifest[c[0]] = run_case(*c)
     manifest["ref16_rerun"] = run_rerun()
+    manifest["readsnap"] = run_readsnap()
     with open(os.path.join(HERE, "manifest.json"), "w") as f:
         json.dump(manifest, f, indent=1)
     print(json.dumps({k: len(v["files"]) for k, v in manifest.items()}))

@@ -555,7 +555,8 @@ def run_ours(args):
     # the 256^3, g = 0 precision config (1000 steps), reported beside the headline
     prec256 = precision_report(256, 0.0, 1000, local) if (args.precision_steps > 0 and N == 512) else None
 
-    batch = {p: run_batch(args, p, local) for p in dict.fromkeys([head, "mixed"])} if args.batch_steps > 0 else None
+    batch = {p: run_batch(args, p, local, args.adjoint_steps if p == head else 0)
+             for p in dict.fromkeys([head, "mixed"])} if args.batch_steps > 0 else None
 
     ic = ic_section(ifdm, args.ic_res, local, 128 if not args.no_cpu_baseline else 0) if (
         args.ic_res > 0 and rank == 0) else None
@@ -643,7 +644,7 @@ def run_ours(args):
         print(json.dumps(out))
 
 
-def run_batch(args, prec, device):
+def run_batch(args, prec, device, adjoint_steps=0):
     """96 realisations of uneven sizes (32 at 32^3, 32 at 48^3, 24 at 64^3, 8 at
     96^3), each with its own seed and mfdm ~ U[1e-24, 5e-24] eV, g = 0, K steps
     with per-box step scales under which 500 kinetic-limited steps would reach
@@ -705,6 +706,35 @@ def run_batch(args, prec, device):
                    for x, y in zip(xs, ys))
 
     a_end = min(sim.state()["a"] for sim in sims)
+    adj = None
+    if adjoint_steps > 0:
+        # batched adjoint (record + backward sweep of every box side by side)
+        # against the boxes' own record + adjoint calls one after another;
+        # host cotangents in and gradients out in both
+        grng = np.random.default_rng(5000)
+        gfin = [grng.standard_normal((n,) * 3) + 1j * grng.standard_normal((n,) * 3) for n in sizes]
+        g0b = [np.empty((n,) * 3, dtype=np.complex128) for n in sizes]
+        g0s = [np.empty((n,) * 3, dtype=np.complex128) for n in sizes]
+        ba = ifdm.Batch(sims)
+        # untimed warm-up of both legs: the first record allocates each box's
+        # checkpoint and segment buffers
+        reset()
+        ba.record_steps(adjoint_steps, dts, 20)
+        ba.adjoint(gfin, g0b)
+        reset()
+        t0 = time.perf_counter()
+        ba.record_steps(adjoint_steps, dts, 20)
+        ba.adjoint(gfin, g0b)
+        t_badj = time.perf_counter() - t0
+        ba.close()
+        reset()
+        t0 = time.perf_counter()
+        for sim, dt, gf, g in zip(sims, dts, gfin, g0s):
+            sim.record_steps(adjoint_steps, dt, 20)
+            sim.adjoint(gf, g)
+        t_sadj = time.perf_counter() - t0
+        adj = {"steps": adjoint_steps, "checkpoint_every": 20, "batch_s": t_badj, "one_at_a_time_s": t_sadj,
+               "speedup": t_sadj / t_badj, "identical": all(np.array_equal(x, y) for x, y in zip(g0b, g0s))}
     for sim in sims:
         sim.close()
     cells = float(sum(n ** 3 for n in sizes))
@@ -715,7 +745,7 @@ def run_batch(args, prec, device):
                                             "tuned_plans": max_rel(out_batch, single)},
             "density_rel_l2_vs_one_at_a_time": {"default_plans": max_rel_rho(out_default, single),
                                                 "tuned_plans": max_rel_rho(out_batch, single)},
-            "min_a_end": a_end, "tuning": tuning,
+            "min_a_end": a_end, "tuning": tuning, "adjoint": adj,
             "items_per_step": info["items_per_step"], "persistent_ctas": info["grid"],
             "note": "wall clock around one graph replay (state reset between runs, graph captured beforehand)"}
 

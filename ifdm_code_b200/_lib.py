@@ -30,7 +30,7 @@ EXPORTS = [
     "ifdm_flush_snapshots", "ifdm_set_snapshot_streaming", "ifdm_snapshots_written", "ifdm_synchronize", "ifdm_stream",
     "ifdm_profile_passes", "ifdm_pass_bytes", "ifdm_fft3d", "ifdm_poisson_static", "ifdm_record_steps",
     "ifdm_adjoint", "ifdm_batch_create", "ifdm_batch_step", "ifdm_batch_tune", "ifdm_batch_get_tuning",
-    "ifdm_batch_set_tuning", "ifdm_batch_synchronize", "ifdm_batch_info", "ifdm_batch_last_error",
+    "ifdm_batch_set_tuning", "ifdm_batch_synchronize", "ifdm_batch_record_steps", "ifdm_batch_adjoint", "ifdm_batch_info", "ifdm_batch_last_error",
     "ifdm_batch_destroy",
 ]
 
@@ -117,6 +117,8 @@ def load_library() -> C.CDLL:
     lib.ifdm_batch_get_tuning.argtypes = [P, C.POINTER(BatchTuning)]
     lib.ifdm_batch_set_tuning.argtypes = [P, C.POINTER(BatchTuning)]
     lib.ifdm_batch_synchronize.argtypes = [P]
+    lib.ifdm_batch_record_steps.argtypes = [P, C.c_int, D, C.c_int]
+    lib.ifdm_batch_adjoint.argtypes = [P, C.POINTER(C.c_void_p), C.POINTER(C.c_void_p)]
     lib.ifdm_batch_info.argtypes = [P, C.POINTER(C.c_longlong), C.POINTER(C.c_int)]
     lib.ifdm_batch_last_error.argtypes = [P]
     lib.ifdm_batch_last_error.restype = C.c_char_p

@@ -145,6 +145,16 @@ __global__ void __launch_bounds__(TileZ<R, K, N>::NT)
     }
 }
 
+// max |x_i| over n doubles into *out (the ordered bits of a non-negative
+// double; *out zeroed before); NaN entries are skipped
+__global__ void k_absmax(const double *__restrict__ x, size_t n, unsigned long long *__restrict__ out) {
+    double m = 0.0;
+    for (size_t i = size_t(blockIdx.x) * blockDim.x + threadIdx.x; i < n; i += size_t(gridDim.x) * blockDim.x)
+        m = fmax(m, fabs(x[i]));
+    m = warp_max(m);
+    if ((threadIdx.x & 31) == 0) atomic_max_nonneg(out, m);
+}
+
 // complex128 (natural units) <-> storage type, with a real scale
 template <typename R>
 __global__ void k_scale_in(const double2 *__restrict__ in, cx<R> *__restrict__ out, double f, size_t n) {

@@ -9,6 +9,7 @@
 #include <cstring>
 #include <memory>
 #include <string>
+#include <thread>
 #include <vector>
 
 #include "batch_engine.hpp"
@@ -487,26 +488,22 @@ int ifdm_adjoint(ifdm_ctx *c, const double *g_final, double *g0) {
     if (c->eng.recorded_steps() <= 0) return fail(c, IFDM_ERR_STATE, "ifdm_adjoint: no recorded steps");
     const size_t bytes = c->eng.n3() * 2 * sizeof(double);
     const bool din = is_device_ptr(g_final), dout = is_device_ptr(g0);
-    double *tin = nullptr, *tout = nullptr;
-    if (!din) {
-        CTX_CUDA(c, cudaMalloc(&tin, bytes));
-        CTX_CUDA(c, cudaMemcpyAsync(tin, g_final, bytes, cudaMemcpyHostToDevice, c->stream));
+    // host arrays go through the context's complex128 staging buffer, in and
+    // out alike: the sweep reads the cotangent at its start and writes the
+    // gradient at its end, so one buffer serves both, and no allocation (which
+    // would synchronise the device) happens per call
+    if (!din || !dout) {
+        if (ensure_out(c)) return IFDM_ERR_CUDA;
+        if (c->snap.ready()) CTX_STR(c, IFDM_ERR_CUDA, c->snap.before_stage(c->stream));
     }
-    if (!dout) {
-        if (cudaMalloc(&tout, bytes) != cudaSuccess) {
-            cudaFree(tin);
-            return fail(c, IFDM_ERR_CUDA, "ifdm_adjoint: device buffer allocation failed");
-        }
-    }
-    std::string e = c->eng.adjoint(din ? g_final : tin, dout ? g0 : tout);
+    if (!din) CTX_CUDA(c, cudaMemcpyAsync(c->d_out, g_final, bytes, cudaMemcpyHostToDevice, c->stream));
+    std::string e = c->eng.adjoint(din ? g_final : c->d_out, dout ? g0 : c->d_out);
     if (e.empty() && !dout) {
-        cudaError_t ce = cudaMemcpyAsync(g0, tout, bytes, cudaMemcpyDeviceToHost, c->stream);
+        cudaError_t ce = cudaMemcpyAsync(g0, c->d_out, bytes, cudaMemcpyDeviceToHost, c->stream);
         if (ce != cudaSuccess) e = std::string("cudaMemcpyAsync: ") + cudaGetErrorString(ce);
     }
     cudaError_t ce = cudaStreamSynchronize(c->stream);
     if (e.empty() && ce != cudaSuccess) e = std::string("cudaStreamSynchronize: ") + cudaGetErrorString(ce);
-    cudaFree(tin);
-    cudaFree(tout);
     if (!e.empty()) return fail(c, IFDM_ERR_CUDA, e);
     TState t{};
     CTX_STR(c, IFDM_ERR_CUDA, c->eng.read_state(t));
@@ -609,6 +606,42 @@ int ifdm_batch_synchronize(ifdm_batch *b) {
     if (!e.empty()) return bfail(b, IFDM_ERR_CUDA, e);
     if (st) return bfail(b, IFDM_ERR_DEVICE, "batch: a dependency wait of the batch kernel gave up");
     return IFDM_OK;
+}
+
+}  // extern "C"
+
+// fn(i) for every context of the batch, on up to 16 host threads at a time;
+// each context works on its own stream, so the boxes' kernels overlap on the
+// device.  Returns the first failing context's code (its message copied).
+template <class F> static int for_each_box(ifdm_batch *b, F fn) {
+    const int n = (int)b->ctx.size();
+    std::vector<int> rc(n, IFDM_OK);
+    const int width = std::min(n, 16);
+    std::vector<std::thread> pool;
+    for (int w = 0; w < width; ++w)
+        pool.emplace_back([&, w] {
+            cudaSetDevice(b->ctx[0]->p.device);
+            for (int i = w; i < n; i += width) rc[i] = fn(i);
+        });
+    for (auto &t : pool) t.join();
+    for (int i = 0; i < n; ++i)
+        if (rc[i] != IFDM_OK) return bfail(b, rc[i], "box " + std::to_string(i) + ": " + b->ctx[i]->err);
+    return IFDM_OK;
+}
+
+extern "C" {
+
+int ifdm_batch_record_steps(ifdm_batch *b, int nsteps, const double *dt_scale, int checkpoint_every) {
+    if (!b || nsteps <= 0 || !dt_scale || checkpoint_every <= 0) return IFDM_ERR_ARGS;
+    return for_each_box(b, [&](int i) {
+        const int rc = ifdm_record_steps(b->ctx[i], nsteps, dt_scale[i], checkpoint_every);
+        return rc ? rc : ifdm_synchronize(b->ctx[i]);
+    });
+}
+
+int ifdm_batch_adjoint(ifdm_batch *b, const double *const *g_final, double *const *g0) {
+    if (!b || !g_final || !g0) return IFDM_ERR_ARGS;
+    return for_each_box(b, [&](int i) { return ifdm_adjoint(b->ctx[i], g_final[i], g0[i]); });
 }
 
 int ifdm_batch_info(ifdm_batch *b, long long *items_per_step, int *grid) {

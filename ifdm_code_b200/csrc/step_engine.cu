@@ -314,6 +314,7 @@ StepEngine::~StepEngine() {
     cudaFree(drift64_);
     cudaFree(drift32_);
     cudaFree(ts_);
+    cudaFree(gmax_);
     cudaFree(part_);
     cudaFree(log_);
     cudaFree(ckpt_psi_);
@@ -601,6 +602,7 @@ std::string StepEngine::ensure_adjoint_buffers(int nsteps, int ckpt) {
         CUDA_TRY(cudaMalloc(&pw_, n3 * rs));
         CUDA_TRY(cudaMalloc(&ts_adj_, sizeof(TState)));
         CUDA_TRY(cudaMemsetAsync(ts_adj_, 0, sizeof(TState), stream_));
+        CUDA_TRY(cudaMalloc(&gmax_, sizeof(unsigned long long)));
         CUDA_TRY(cudaMalloc(&drift64_adj_, sizeof(double2) * cfg_.N));
         CUDA_TRY(cudaMalloc(&drift32_adj_, sizeof(float2) * cfg_.N));
         if (use_tma_) {
@@ -670,11 +672,29 @@ std::string StepEngine::adjoint(const double *g_final_dev, double *g0_dev) {
     TState fin{};
     CUDA_TRY(cudaMemcpyAsync(&fin, ts_, sizeof(TState), cudaMemcpyDeviceToHost, stream_));
     CUDA_TRY(cudaStreamSynchronize(stream_));
-    // natural units -> gradient with respect to the stored (scaled) field: g_s = S g
+    // natural units -> gradient with respect to the stored (scaled) field:
+    // g_s = S g.  S ~ 1e50, so in FP32 storage S g overflows for any
+    // cotangent of order one; the sweep is linear in g, so FP32 and mixed
+    // carry lambda S g with a power of two lambda that brings max|lambda S g|
+    // into [1, 2) (a power of two changes no rounding) and divide it out at
+    // the end.  FP64 keeps lambda = 1.
+    double lambda = 1.0;
+    if (cfg_.precision != 0) {
+        CUDA_TRY(cudaMemsetAsync(gmax_, 0, sizeof(unsigned long long), stream_));
+        k_absmax<<<1184, 256, 0, stream_>>>(g_final_dev, 2 * n3, gmax_);
+        CUDA_TRY(cudaGetLastError());
+        unsigned long long bits = 0;
+        CUDA_TRY(cudaMemcpyAsync(&bits, gmax_, sizeof(bits), cudaMemcpyDeviceToHost, stream_));
+        CUDA_TRY(cudaStreamSynchronize(stream_));
+        double gmax = 0.0;
+        std::memcpy(&gmax, &bits, sizeof(gmax));
+        const double top = gmax * S_;
+        if (top > 0.0 && std::isfinite(top)) lambda = std::ldexp(1.0, -std::ilogb(top));
+    }
     if (cfg_.precision == 0)
         k_scale_in<double><<<1184, 256, 0, stream_>>>((const double2 *)g_final_dev, (double2 *)g_, S_, n3);
     else
-        k_scale_in<float><<<1184, 256, 0, stream_>>>((const double2 *)g_final_dev, (float2 *)g_, S_, n3);
+        k_scale_in<float><<<1184, 256, 0, stream_>>>((const double2 *)g_final_dev, (float2 *)g_, S_ * lambda, n3);
     CUDA_TRY(cudaGetLastError());
     // the output map: psi_out = S psi exp(-i (pendP phi + pendQ |psi|^2 - gphase))
     std::string e = adjoint_kick(psi_, phi_, fin.pendP, fin.pendP, fin.pendQ, -fin.gphase, 1ll << 40);
@@ -726,7 +746,8 @@ std::string StepEngine::adjoint(const double *g_final_dev, double *g0_dev) {
     if (cfg_.precision == 0)
         k_scale_out<double><<<1184, 256, 0, stream_>>>((const double2 *)g_, (double2 *)g0_dev, 1.0 / S_, n3);
     else
-        k_scale_out<float><<<1184, 256, 0, stream_>>>((const float2 *)g_, (double2 *)g0_dev, 1.0 / S_, n3);
+        k_scale_out<float><<<1184, 256, 0, stream_>>>((const float2 *)g_, (double2 *)g0_dev, 1.0 / (S_ * lambda),
+                                                      n3);
     CUDA_TRY(cudaGetLastError());
     recorded_ = 0;  // the replay consumed the state; record again before another adjoint
     return "";

@@ -111,6 +111,7 @@ class StepEngine {
     void *ckpt_psi_ = nullptr, *ckpt_phi_ = nullptr, *seg_psi_ = nullptr, *seg_phi_ = nullptr;
     void *g_ = nullptr, *w_ = nullptr, *pw_ = nullptr;
     TState *ts_adj_ = nullptr;
+    unsigned long long *gmax_ = nullptr;  // max |component| of the incoming gradient (ordered bits)
     double2 *drift64_adj_ = nullptr;
     float2 *drift32_adj_ = nullptr;
     CUtensorMap map_g_y_{}, map_g_x_{};

@@ -373,16 +373,21 @@ __global__ void __launch_bounds__(TileZ<R, K, N>::NT)
     fft_tile<C, M, TL::EHD, +1, TL::L, TL::LP>(sm, twh);
     const K *smr = reinterpret_cast<const K *>(sm);
     constexpr KSplit<K> inv(1.0 / ((double)N * N * N));
-    double mx = 0.0;
+    R *out = phi + row0 * N;
+    // max|phi| over the reference's scan window: element f of the tile is in
+    // it when (row0 + f / N) * N + f % N < win_rows * N + win_tail, one
+    // comparison against a per-tile limit (the loop is integer-bound otherwise)
+    const bool inside = (long)(row0 + TL::L) <= win_rows;
+    const int lim = inside ? TL::L * N : (int)max(0L, min((long)TL::L * N, (win_rows - (long)row0) * N + win_tail));
+    R mx = R(0);
     for (int f = threadIdx.x; f < TL::L * N; f += TL::NT) {
         const int l = f / N, n = f % N;
         const R v = Cvt<R, K>::outr(mulk(smr[2 * ((n >> 1) * TL::LP + l) + (n & 1)], inv.hi, inv.lo), salt, row0 * N + f);
-        phi[row0 * N + f] = v;
-        const long row = (long)(row0 + l);
-        if (row < win_rows || (row == win_rows && n < win_tail)) mx = fmax(mx, (double)fabs(v));
+        out[f] = v;
+        if (f < lim) mx = fmax(mx, fabs(v));
     }
-    mx = warp_max(mx);
-    if ((threadIdx.x & 31) == 0) atomic_max_nonneg(&ts->maxphi_bits, mx);
+    const double m = warp_max((double)mx);
+    if ((threadIdx.x & 31) == 0) atomic_max_nonneg(&ts->maxphi_bits, m);
 }
 
 // --------------------------------------------------------- y / x passes ---

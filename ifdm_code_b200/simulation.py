@@ -266,6 +266,24 @@ class Batch:
         return {"mode": t.mode, "blocks_per_sm": t.blocks_per_sm, "group": t.group, "plan": list(t.plan),
                 "ms_per_step": t.ms_per_step}
 
+    def record_steps(self, nsteps: int, dt_scale=1.0, checkpoint_every: int = 20) -> None:
+        """Every box records nsteps fixed-mode steps for its adjoint, the boxes
+        side by side (each on its own stream)."""
+        self._c(self.lib.ifdm_batch_record_steps(self.h, nsteps, self._dts(dt_scale), checkpoint_every))
+
+    def adjoint(self, g_finals, g0s) -> None:
+        """The adjoint of every box's recorded steps, side by side; g_finals /
+        g0s: one complex128 array (numpy or CUDA tensor) per box."""
+        if len(g_finals) != len(self.sims) or len(g0s) != len(self.sims):
+            raise ValueError("one g_final and one g0 per box")
+
+        def ptr(a):
+            return a.data_ptr() if hasattr(a, "data_ptr") else a.ctypes.data
+
+        gin = (C.c_void_p * len(self.sims))(*[ptr(a) for a in g_finals])
+        gout = (C.c_void_p * len(self.sims))(*[ptr(a) for a in g0s])
+        self._c(self.lib.ifdm_batch_adjoint(self.h, gin, gout))
+
     def info(self) -> dict:
         items, grid = C.c_longlong(), C.c_int()
         self._c(self.lib.ifdm_batch_info(self.h, C.byref(items), C.byref(grid)))

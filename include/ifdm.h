@@ -207,6 +207,13 @@ int ifdm_batch_get_tuning(ifdm_batch *b, ifdm_batch_tuning *out);
 int ifdm_batch_set_tuning(ifdm_batch *b, const ifdm_batch_tuning *t);
 /* Wait for the batch; IFDM_ERR_DEVICE if a dependency wait gave up. */
 int ifdm_batch_synchronize(ifdm_batch *b);
+/* Batched adjoint: ifdm_record_steps / ifdm_adjoint of every box, the boxes
+ * side by side (one host thread and the box's own stream each, up to 16 at a
+ * time), so many small boxes fill the GPU together.  dt_scale, g_final and g0
+ * have one entry per box (host or device complex128 N_i^3 arrays).  Results
+ * equal the boxes' own ifdm_adjoint calls bit for bit. */
+int ifdm_batch_record_steps(ifdm_batch *b, int nsteps, const double *dt_scale, int checkpoint_every);
+int ifdm_batch_adjoint(ifdm_batch *b, const double *const *g_final, double *const *g0);
 /* Work items of one batch step and the persistent CTAs of all sizes. */
 int ifdm_batch_info(ifdm_batch *b, long long *items_per_step, int *grid);
 const char *ifdm_batch_last_error(const ifdm_batch *b);

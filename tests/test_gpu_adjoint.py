@@ -116,3 +116,31 @@ def test_reduced_precision_adjoint_close_to_fp64():
     for prec, tol in (("mixed", 1e-4), ("fp32", 1e-3)):
         e = np.linalg.norm(grads[prec] - grads["fp64"]) / np.linalg.norm(grads["fp64"])
         assert e <= tol, (prec, e)
+
+
+def test_reduced_precision_adjoint_of_any_cotangent_scale():
+    # The sweep works on the gradient of the stored field, S g with S ~ 1e50;
+    # FP32 storage would overflow for a cotangent of order one, so FP32 and
+    # mixed carry it scaled by a power of two.  Gradients are finite, scale
+    # exactly with the cotangent, and agree with FP64.
+    n, nsteps, C = 32, 6, 0.05
+    psi0 = zeldovich_psi(n, seed=11)
+    rng = np.random.default_rng(3)
+    gfin = rng.standard_normal((n,) * 3) + 1j * rng.standard_normal((n,) * 3)
+
+    def grad(prec, g):
+        with ifdm.Simulation(MFDM, 0.0, XMAX, n, precision=prec) as sim:
+            sim.set_psi(psi0, A0)
+            sim.record_steps(nsteps, C, 3)
+            out = np.empty_like(g)
+            sim.adjoint(g, out)
+        return out
+
+    ref = grad("fp64", gfin)
+    for prec, tol in (("mixed", 1e-4), ("fp32", 1e-3)):
+        g1 = grad(prec, gfin)
+        g2 = grad(prec, gfin * 2.0**-60)
+        assert np.isfinite(g1).all(), prec
+        assert np.array_equal(g2 * 2.0**60, g1), prec
+        e = np.linalg.norm(g1 - ref) / np.linalg.norm(ref)
+        assert e <= tol, (prec, e)

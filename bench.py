@@ -828,6 +828,7 @@ def main():
     ap.add_argument("--res", type=int, default=N_DEFAULT)
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--profile", action="store_true", help="plain W+K steps of --precision (for ncu)")
+    ap.add_argument("--profile-ic", action="store_true", help="only the IC section at --ic-res (for ncu)")
     ap.add_argument("--calibrate-g", action="store_true", help="print the g of the self-interaction config")
     ap.add_argument("--precision", choices=["fp32", "fp64", "mixed"], default="mixed")
     ap.add_argument("--adjoint-steps", type=int, default=40, help="steps of the adjoint timing (0 skips it)")
@@ -850,6 +851,10 @@ def main():
         args.warmup = 3
     if args.profile:
         run_profile(args)
+    elif args.profile_ic:
+        import ifdm_code_b200 as ifdm
+
+        print(json.dumps(ic_section(ifdm, args.ic_res, 0, 0)))
     elif args.calibrate_g:
         calibrate_g(args)
     elif args.impl == "reference":

@@ -14,6 +14,7 @@ import os
 import shutil
 import subprocess
 import sys
+import time
 
 PKG = os.path.dirname(os.path.abspath(__file__))
 ROOT = os.path.dirname(PKG)
@@ -94,8 +95,16 @@ def build(force: bool = False, verbose: bool = False) -> str:
         objs.append(out)
         if force or _stale(out, src, hdr):
             jobs.append(["g++"] + CXX_FLAGS + ["-I" + os.path.join(cuda, "include"), "-c", src, "-o", out])
+    # an object is stamped with the time its compile started, so a source or
+    # header edited while it compiled stays newer than it and is rebuilt next time
+    t_start = time.time()
+
+    def compile_one(cmd):
+        _run(cmd, verbose)
+        os.utime(cmd[cmd.index("-o") + 1], (t_start, t_start))
+
     with cf.ThreadPoolExecutor(max_workers=max(1, min(len(jobs), os.cpu_count() or 1))) as ex:
-        list(ex.map(lambda c: _run(c, verbose), jobs))
+        list(ex.map(compile_one, jobs))
     if force or jobs or not os.path.exists(LIB):
         _run([nvcc] + ARCH + ["-shared", "-ccbin", "g++", "-o", LIB] + objs + ["-lcudart_static", "-lrt", "-ldl"],
              verbose)

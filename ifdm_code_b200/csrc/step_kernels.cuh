@@ -379,12 +379,19 @@ __global__ void __launch_bounds__(TileZ<R, K, N>::NT)
     // comparison against a per-tile limit (the loop is integer-bound otherwise)
     const bool inside = (long)(row0 + TL::L) <= win_rows;
     const int lim = inside ? TL::L * N : (int)max(0L, min((long)TL::L * N, (win_rows - (long)row0) * N + win_tail));
-    R mx = R(0);
+    // the running max on the pipe the pass leaves idle: FP64 for FP32, whose
+    // integer pipe is the busy one (measured at 512^3: 0.53 ms with a
+    // per-element window test and an FP64 max, 0.60 with the tile limit and a
+    // float max, 0.45 with the tile limit and an FP64 max); the storage type
+    // for FP64 and mixed, whose FP64 pipe is busy (0.67 -> 0.64 and
+    // 0.73 -> 0.65 ms)
+    using MX = std::conditional_t<sizeof(K) == 4, double, R>;
+    MX mx = MX(0);
     for (int f = threadIdx.x; f < TL::L * N; f += TL::NT) {
         const int l = f / N, n = f % N;
         const R v = Cvt<R, K>::outr(mulk(smr[2 * ((n >> 1) * TL::LP + l) + (n & 1)], inv.hi, inv.lo), salt, row0 * N + f);
         out[f] = v;
-        if (f < lim) mx = fmax(mx, fabs(v));
+        if (f < lim) mx = fmax(mx, (MX)fabs(v));
     }
     const double m = warp_max((double)mx);
     if ((threadIdx.x & 31) == 0) atomic_max_nonneg(&ts->maxphi_bits, m);

@@ -114,7 +114,7 @@ __global__ void __launch_bounds__(TmaTile<R, K, N, AXIS>::NT, 1)
         stage_load<C, N, E, L, L, R0>(land, v, l, t);
         if constexpr (TL::OWN_WORK) fence_proxy_async_smem();  // slot is released at the next barrier
         stage_compute<C, N, E, (MODE == 0 ? DIR : -1), R0, 1>(v, tw, t);
-        RegChain<C, N, E, (MODE == 0 ? DIR : -1), L, LPW, 1, R0>::run(wk, v, tw, l, t, true);
+        RegChain<C, N, E, (MODE == 0 ? DIR : -1), L, LPW, 1, R0, TL::NARROW>::run(wk, v, tw, l, t, true);
         if (MODE != 0) {
             // v[b*RL + r] holds element n = (t + T*b) + r*N/RL of the forward transform
             if (MODE == 1) {
@@ -147,7 +147,7 @@ __global__ void __launch_bounds__(TmaTile<R, K, N, AXIS>::NT, 1)
                         v[b * RL + r] = cscale(v[b * RL + r], k2 == 0 ? K(0) : K(-1) / K(k2));
                     }
             }
-            fft_regs_chained<C, N, E, +1, L, LPW>(wk, v, tw, l, t, true);
+            fft_regs_chained<C, N, E, +1, L, LPW, TL::NARROW>(wk, v, tw, l, t, true);
         }
         if ((g % W) < VW) {
             const size_t b0 = AXIS == 1 ? size_t(g / W) * N * W + size_t(g % W) : size_t(g);

@@ -7,11 +7,12 @@ Workload (ours): one 512^3 box (xmax = 5 Mpc/h, mfdm = 2.5e-24 eV, g = 0) from a
 seeded z = 50 Zel'dovich field, fixed-step mode with the reference's timestep
 rule scaled so 1000 steps reach a = 0.5.  A "step" is one full leap-frog step
 (timestep + kick + FFT + drift + iFFT + Poisson + kick, 10 kernels).  The
-headline `value` is the FP32-mixed path with psi resident in HBM; the FP64
-(drop-in) path is timed the same way beside it.  `e2e` times the public API
+headline `value` is the fastest path (FP32, mixed or FP64) whose density stays
+within 1e-5 of FP64 after 1000 steps, with psi resident in HBM; every path is
+timed the same way beside it.  `e2e` times the public API
 with host buffers: psi uploaded from pinned memory, K steps, psi read back.
-With --gpus N > 1 (torchrun) every rank advances its own box (replicas: the
-north star keeps one box per GPU), timed as the max over ranks.
+With --gpus N > 1 (torchrun) every rank advances its own box (replicas: one
+box per GPU, no exchange between them), timed as the max over ranks.
 
 --impl reference times the reference's own CPU code (oracle/_ref/BECMPI_ref,
 its unmodified sources with single-rank MPI/FFTW/GSL shims) on this host:

@@ -210,8 +210,9 @@ __global__ void __launch_bounds__(TileZ<R, K, N>::NT)
         // mixed: all of this thread's loads first (PER of psi and of phi in
         // flight), then the kicks (measured at 512^3: 1.42 -> 1.19 ms; in FP64
         // and FP32 the extra registers cost a resident block and it was slower,
-        // and so was loading the whole psi and phi tile into shared memory
-        // with cp.async first: FP32 0.77 -> 0.83 ms, FP64 1.45 -> 1.53 ms)
+        // and so were loading the whole psi and phi tile into shared memory
+        // with cp.async first (FP32 0.77 -> 0.83 ms, FP64 1.45 -> 1.53 ms) and
+        // unrolling the FP32 loop by two under a 32-register cap (0.76 -> 0.81 ms))
         constexpr int PER = TL::L * N / TL::NT;
         static_assert(PER * TL::NT == TL::L * N, "whole rows per thread block");
         typename TL::G g[PER];

@@ -93,11 +93,11 @@ def zeldovich_particles(N: int, xmax: float = 5.0, seed: int = 0, a: float = 1.0
     amp = k2 ** (slope / 4.0)
     amp[0, 0, 0] = 0.0
     dk = wk * amp
-    delta = np.fft.irfftn(dk, s=(N, N, N))
+    delta = np.fft.irfftn(dk, s=(N, N, N), axes=(0, 1, 2))
     dk *= rms_delta / delta.std()
     disp = []
     for kc in (kx, ky, kz):
-        disp.append(np.fft.irfftn(1j * kc / k2 * dk, s=(N, N, N)))
+        disp.append(np.fft.irfftn(1j * kc / k2 * dk, s=(N, N, N), axes=(0, 1, 2)))
     q = (np.arange(N) + 0.5) * Lg
     qx, qy, qz = np.meshgrid(q, q, q, indexing="ij")
     E = np.sqrt(OMEGA_M0 / a**3 + 1.0 - OMEGA_M0)

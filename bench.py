@@ -150,24 +150,6 @@ def time_steps(sim, steps: int, warmup: int, dt_scale: float, torch):
     return e0.elapsed_time(e1)
 
 
-def power_spectrum(rho, nbins: int = 24):
-    """Spherically averaged P(k) of the density contrast, log-spaced |k| bins."""
-    import numpy as np
-    import scipy.fft as sfft
-
-    N = rho.shape[0]
-    d = rho / rho.mean() - 1.0
-    pk = np.abs(sfft.rfftn(d, workers=-1)) ** 2
-    k = np.fft.fftfreq(N) * N
-    kr = np.fft.rfftfreq(N) * N
-    kk = np.sqrt(k[:, None, None] ** 2 + k[None, :, None] ** 2 + kr[None, None, :] ** 2)
-    edges = np.logspace(0, np.log10(N / 2), nbins + 1)
-    idx = np.digitize(kk.ravel(), edges)
-    sums = np.bincount(idx, weights=pk.ravel(), minlength=nbins + 2)[1:nbins + 1]
-    cnt = np.bincount(idx, minlength=nbins + 2)[1:nbins + 1]
-    return sums[cnt > 0] / cnt[cnt > 0]
-
-
 def g_for_phase(N: int, psi0, dt_scale: float, phase: float) -> float:
     """Self-interaction g [eV cm^3] whose kick turns the densest cell of psi0 by
     `phase` radians in the first step: that turn is dt_QI (g/hbar) max|psi|^2
@@ -233,18 +215,19 @@ def precision_report(N: int, g: float, nsteps: int, device: int, seed: int = 0) 
 
     C = dt_scale_for(N, nsteps)
     psi0 = zeldovich_psi(N, xmax=XMAX, seed=seed, a=A0, mfdm=MFDM)
-    rho = {}
+    rho, pks = {}, {}
     for prec in ("fp64", "mixed", "fp32"):
         with ifdm.Simulation(MFDM, g, XMAX, N, precision=prec, device=device) as sim:
             sim.set_psi(psi0, A0)
             sim.step(nsteps, C)
             rho[prec] = np.abs(sim.get_psi()) ** 2
+            pks[prec] = sim.power_spectrum(24)["pk"]  # on the device (ifdm_power_spectrum)
             a_end = sim.state()["a"]
-    pk_ref = power_spectrum(rho["fp64"])
+    pk_ref = pks["fp64"]
     out = {"res": N, "g": g, "steps": nsteps, "dt_scale": C, "a_end": a_end}
     for prec in ("mixed", "fp32"):
         r, ref = rho[prec], rho["fp64"]
-        ratio = power_spectrum(r) / pk_ref
+        ratio = pks[prec] / pk_ref
         out[prec] = {"density_relL2": float(np.linalg.norm(r - ref) / np.linalg.norm(ref)),
                      "norm_drift": float(r.sum() / ref.sum() - 1.0),
                      "pk_ratio_max_dev": float(np.max(np.abs(ratio - 1.0))),
@@ -480,6 +463,7 @@ def run_ours(args):
             sim.set_psi(psi0, A0)
             sim.step(args.precision_steps, C)
             res[prec]["rho"] = np.abs(sim.get_psi()) ** 2
+            res[prec]["pk"] = sim.power_spectrum(24)["pk"]  # on the device (ifdm_power_spectrum)
             res[prec]["a_end"] = sim.state()["a"]
         sim.close()
         del sim
@@ -487,10 +471,10 @@ def run_ours(args):
     prec_report = {}
     if args.precision_steps > 0:
         ref = res["fp64"]["rho"]
-        pk_ref = power_spectrum(ref)
+        pk_ref = res["fp64"]["pk"]
         for prec in ("mixed", "fp32"):
             rho = res[prec]["rho"]
-            pk = power_spectrum(rho)
+            pk = res[prec]["pk"]
             prec_report[prec] = {
                 "steps": args.precision_steps,
                 "density_relL2": float(np.linalg.norm(rho - ref) / np.linalg.norm(ref)),

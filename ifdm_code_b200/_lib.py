@@ -26,7 +26,7 @@ IC_REF1, IC_EXACT = 0, 1
 EXPORTS = [
     "ifdm_params_default", "ifdm_params_from_argv", "ifdm_create", "ifdm_destroy", "ifdm_last_error",
     "ifdm_supported_res", "ifdm_load_ic", "ifdm_load_snapshot", "ifdm_set_psi", "ifdm_get_psi", "ifdm_get_phi",
-    "ifdm_get_state", "ifdm_power_spectrum", "ifdm_run", "ifdm_step", "ifdm_write_snapshot", "ifdm_write_snapshot_async",
+    "ifdm_get_state", "ifdm_power_spectrum", "ifdm_get_energies", "ifdm_run", "ifdm_step", "ifdm_write_snapshot", "ifdm_write_snapshot_async",
     "ifdm_flush_snapshots", "ifdm_set_snapshot_streaming", "ifdm_snapshots_written", "ifdm_synchronize", "ifdm_stream",
     "ifdm_profile_passes", "ifdm_pass_bytes", "ifdm_fft3d", "ifdm_poisson_static", "ifdm_record_steps",
     "ifdm_adjoint", "ifdm_batch_create", "ifdm_batch_step", "ifdm_batch_tune", "ifdm_batch_get_tuning",
@@ -48,6 +48,11 @@ class Params(C.Structure):
         ("icpath", C.c_char_p), ("rerun", C.c_int), ("precision", C.c_int), ("stan", C.c_int),
         ("ic_mode", C.c_int), ("device", C.c_int), ("verbose", C.c_int),
     ]
+
+
+class Energies(C.Structure):
+    _fields_ = [("mean_rho", C.c_double), ("mean_grad2", C.c_double), ("mean_phi_rho", C.c_double),
+                ("mean_rho2", C.c_double)]
 
 
 class State(C.Structure):
@@ -94,6 +99,7 @@ def load_library() -> C.CDLL:
     lib.ifdm_get_phi.argtypes = [P, C.c_void_p]
     lib.ifdm_get_state.argtypes = [P, C.POINTER(State)]
     lib.ifdm_power_spectrum.argtypes = [P, C.c_int, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p]
+    lib.ifdm_get_energies.argtypes = [P, C.POINTER(Energies)]
     lib.ifdm_run.argtypes = [P]
     lib.ifdm_step.argtypes = [P, C.c_int, C.c_double]
     lib.ifdm_write_snapshot.argtypes = [P, C.c_int]

@@ -169,7 +169,86 @@ void launch_bins(const double2 *rk, int N, int nb, const BinEdges &ed, double *p
     k_bin_lines<PER><<<groups, kBinThreads, 0, s>>>(rk, N, nb, ed, part);
 }
 
+// sums over x of |psi|^2, |psi|^4 and phi |psi|^2: part[3 * block + {0, 1, 2}]
+__global__ void k_xsums(const double2 *__restrict__ psi, const double *__restrict__ phi, size_t n,
+                        double *__restrict__ part) {
+    __shared__ double red[32];
+    double a = 0.0, b = 0.0, c = 0.0;
+    for (size_t i = size_t(blockIdx.x) * blockDim.x + threadIdx.x; i < n; i += size_t(gridDim.x) * blockDim.x) {
+        const double2 v = psi[i];
+        const double r = v.x * v.x + v.y * v.y;
+        a += r;
+        b += r * r;
+        c += phi[i] * r;
+    }
+    a = block_sum(a, red);
+    b = block_sum(b, red);
+    c = block_sum(c, red);
+    if (threadIdx.x == 0) {
+        part[3 * blockIdx.x] = a;
+        part[3 * blockIdx.x + 1] = b;
+        part[3 * blockIdx.x + 2] = c;
+    }
+}
+
+// sum over k of |kappa|^2 |psi_k|^2 (kappa per axis in -N/2 .. N/2-1): part[block]
+__global__ void k_ksum(const double2 *__restrict__ pk, int N, double *__restrict__ part) {
+    __shared__ double red[32];
+    const size_t n3 = size_t(N) * N * N;
+    double a = 0.0;
+    for (size_t i = size_t(blockIdx.x) * blockDim.x + threadIdx.x; i < n3; i += size_t(gridDim.x) * blockDim.x) {
+        const int ix = int(i / (size_t(N) * N)), iy = int((i / N) % N), iz = int(i % N);
+        const double kx = ix < N / 2 ? ix : ix - N, ky = iy < N / 2 ? iy : iy - N, kz = iz < N / 2 ? iz : iz - N;
+        const double2 v = pk[i];
+        a += (kx * kx + ky * ky + kz * kz) * (v.x * v.x + v.y * v.y);
+    }
+    a = block_sum(a, red);
+    if (threadIdx.x == 0) part[blockIdx.x] = a;
+}
+
+// out[c] = sum over blocks b (in order) of part[nv * b + c], c < nv
+__global__ void k_sum_cols(const double *__restrict__ part, int nb, int nv, double *__restrict__ out) {
+    __shared__ double red[32];
+    for (int c = 0; c < nv; ++c) {
+        double a = 0.0;
+        for (int b = threadIdx.x; b < nb; b += blockDim.x) a += part[size_t(nv) * b + c];
+        a = block_sum(a, red);
+        if (threadIdx.x == 0) out[c] = a;
+    }
+}
+
 }  // namespace
+
+std::string field_means(double2 *psi_work, const double *phi, int N, double xmax, double out[4], cudaStream_t s) {
+    if (N < 2 || N > 1024) return "unsupported grid";
+    const size_t n3 = size_t(N) * N * N;
+    double *d_part = nullptr;
+    std::string err;
+    auto run = [&]() -> std::string {
+        DG_TRY(cudaMalloc(&d_part, sizeof(double) * (4 * kSumBlocks + 4)));
+        double *d_tot = d_part + 4 * kSumBlocks;
+        k_xsums<<<kSumBlocks, kSumThreads, 0, s>>>(psi_work, phi, n3, d_part);
+        k_sum_cols<<<1, 1024, 0, s>>>(d_part, kSumBlocks, 3, d_tot);
+        DG_TRY(cudaGetLastError());
+        const std::string e = fft3d(psi_work, N, 0, -1, s);
+        if (!e.empty()) return e;
+        k_ksum<<<kSumBlocks, kSumThreads, 0, s>>>(psi_work, N, d_part + 3 * kSumBlocks);
+        k_sum_cols<<<1, 1024, 0, s>>>(d_part + 3 * kSumBlocks, kSumBlocks, 1, d_tot + 3);
+        DG_TRY(cudaGetLastError());
+        double h[4];
+        DG_TRY(cudaMemcpyAsync(h, d_tot, sizeof(h), cudaMemcpyDeviceToHost, s));
+        DG_TRY(cudaStreamSynchronize(s));
+        const double inv = 1.0 / double(n3), kf = 3.14159265358979323846 / xmax;  // k = pi kappa / xmax
+        out[0] = h[0] * inv;
+        out[1] = h[3] * inv * inv * kf * kf;  // Parseval: sum_x |grad psi|^2 = sum_k k^2 |psi_k|^2 / N^3
+        out[2] = h[2] * inv;
+        out[3] = h[1] * inv;
+        return "";
+    };
+    err = run();
+    cudaFree(d_part);
+    return err;
+}
 
 std::string power_spectrum(double2 *work, int N, double L, int nbins, const double *edges, double *k_out,
                            double *pk_out, long long *modes_out, double *mean_rho, cudaStream_t s) {

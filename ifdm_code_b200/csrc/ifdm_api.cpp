@@ -35,6 +35,7 @@ struct ifdm_ctx {
     StepEngine eng;
     bool have_psi = false;
     double *d_out = nullptr;   // complex128 N^3 device staging for outputs
+    double *d_phi = nullptr;   // N^3 doubles of phi for the field means (first use)
     double *h_out = nullptr;   // pinned host staging
     size_t h_out_bytes = 0;
     bool stream_snapshots = true;  // snapshots copied and written beside the steps
@@ -138,6 +139,7 @@ void ifdm_destroy(ifdm_ctx *c) {
     c->snap.drain();
     if (c->stream) cudaStreamSynchronize(c->stream);
     cudaFree(c->d_out);
+    cudaFree(c->d_phi);
     if (c->h_out) cudaFreeHost(c->h_out);
     if (c->stream) cudaStreamDestroy(c->stream);
     delete c;
@@ -219,6 +221,23 @@ int ifdm_power_spectrum(ifdm_ctx *c, int nbins, const double *edges, double *k, 
     CTX_STR(c, IFDM_ERR_CUDA, c->eng.psi_out(c->d_out, 2));
     CTX_STR(c, IFDM_ERR_ARGS, power_spectrum(reinterpret_cast<double2 *>(c->d_out), c->N, 2.0 * c->xmax, nbins, edges,
                                              k, pk, modes, mean_rho, c->stream));
+    return IFDM_OK;
+}
+
+int ifdm_get_energies(ifdm_ctx *c, ifdm_energies *out) {
+    if (!c || !out) return IFDM_ERR_ARGS;
+    if (!c->have_psi) return fail(c, IFDM_ERR_STATE, "no wave function loaded");
+    if (ensure_out(c)) return IFDM_ERR_CUDA;
+    if (!c->d_phi) CTX_CUDA(c, cudaMalloc(&c->d_phi, c->eng.n3() * sizeof(double)));
+    if (c->snap.ready()) CTX_STR(c, IFDM_ERR_CUDA, c->snap.before_stage(c->stream));
+    CTX_STR(c, IFDM_ERR_CUDA, c->eng.phi_out(c->d_phi));
+    CTX_STR(c, IFDM_ERR_CUDA, c->eng.psi_out(c->d_out, 2));
+    double m[4];
+    CTX_STR(c, IFDM_ERR_CUDA, field_means(reinterpret_cast<double2 *>(c->d_out), c->d_phi, c->N, c->xmax, m, c->stream));
+    out->mean_rho = m[0];
+    out->mean_grad2 = m[1];
+    out->mean_phi_rho = m[2];
+    out->mean_rho2 = m[3];
     return IFDM_OK;
 }
 

@@ -14,7 +14,7 @@ import ctypes as C
 import numpy as np
 
 from . import _lib
-from ._lib import BatchTuning, IfdmError, Params, State
+from ._lib import BatchTuning, Energies, IfdmError, Params, State
 
 
 def _check(lib, h, rc: int) -> int:
@@ -135,6 +135,13 @@ class Simulation:
                                              k.ctypes.data_as(C.c_void_p), pk.ctypes.data_as(C.c_void_p),
                                              modes.ctypes.data_as(C.c_void_p), C.byref(mean)))
         return {"k": k, "pk": pk, "modes": modes, "mean_rho": mean.value}
+
+    def energies(self) -> dict:
+        """Grid means of the current state, on the device: <|psi|^2>,
+        <|grad psi|^2> (1/Mpc^2 x psi units), <phi |psi|^2> and <|psi|^4>."""
+        e = Energies()
+        self._c(self.lib.ifdm_get_energies(self.h, C.byref(e)))
+        return {k: getattr(e, k) for k, _ in Energies._fields_}
 
     def state(self) -> dict:
         s = State()

@@ -124,6 +124,18 @@ int ifdm_get_state(ifdm_ctx *ctx, ifdm_state *out);
  * nbins <= 64.  Every sum has a fixed order: repeated calls agree bit for bit. */
 int ifdm_power_spectrum(ifdm_ctx *ctx, int nbins, const double *edges, double *k, double *pk, long long *modes,
                         double *mean_rho);
+/* Grid means of the current state for energy bookkeeping, computed on the
+ * device (an extension: the reference has no such output), in the natural
+ * units of ifdm_get_psi / ifdm_get_phi: the energy densities are
+ * hbar^2/(2m) mean_grad2 (kinetic), m mean_phi_rho / 2 (gravitational) and
+ * g mean_rho2 / 2 (self-interaction).  Fixed-order sums. */
+typedef struct ifdm_energies {
+    double mean_rho;     /* <|psi|^2> */
+    double mean_grad2;   /* <|grad psi|^2>, spectral derivative, k = pi kappa / xmax [1/Mpc] */
+    double mean_phi_rho; /* <phi |psi|^2> */
+    double mean_rho2;    /* <|psi|^4> */
+} ifdm_energies;
+int ifdm_get_energies(ifdm_ctx *ctx, ifdm_energies *out);
 
 /* Simulation (src/CosmoBEC_MPI.cpp:183-310): steps ti..t_stop-1 with the
  * adaptive timestep, the snapshot state machine and its early stops. */

@@ -80,3 +80,25 @@ def test_power_spectrum_after_steps_and_arguments(tmp_path):
     _, pk, cnt, _ = numpy_pk(now, edges, 2 * XMAX / H)
     np.testing.assert_array_equal(got["modes"], cnt)
     np.testing.assert_allclose(got["pk"], pk, rtol=1e-10)
+
+
+@pytest.mark.parametrize("prec", ["fp64", "fp32"])
+def test_field_means_match_numpy(tmp_path, prec):
+    # grid means for the energy terms against numpy on the state the library
+    # reports (get_psi / get_phi): FP64 sums on both sides
+    N = 32
+    psi0 = zeldovich_psi(N, xmax=XMAX, seed=5, a=1 / 51, mfdm=MFDM)
+    with Simulation(MFDM, 0.0, XMAX, N, opath=str(tmp_path) + "/", precision=prec) as s:
+        s.set_psi(psi0, 1 / 51)
+        s.step(4, 0.1)
+        psi, phi = s.get_psi(), s.get_phi()
+        got = s.energies()
+        again = s.energies()
+    rho = np.abs(psi) ** 2
+    kap = np.fft.fftfreq(N) * N
+    k2 = (kap[:, None, None] ** 2 + kap[None, :, None] ** 2 + kap[None, None, :] ** 2) * (np.pi / (XMAX / H)) ** 2
+    want = {"mean_rho": rho.mean(), "mean_rho2": (rho ** 2).mean(), "mean_phi_rho": (phi * rho).mean(),
+            "mean_grad2": float((k2 * np.abs(np.fft.fftn(psi)) ** 2).sum()) / N ** 6}
+    for k, v in want.items():
+        assert got[k] == pytest.approx(v, rel=1e-12), k
+    assert got == again

@@ -91,55 +91,64 @@ std::string ic_scan_chunks(const std::string &icpath, int nchunks, int N, bool r
     return "";
 }
 
-static std::string upload_chunk(const IcChunk &ch, bool ref1, float *d_pos, float *d_vel, int device,
-                                size_t piece) {
+namespace {
+
+// a contiguous byte range of one chunk's position or velocity block and its
+// place in the device arrays
+struct Range {
+    int chunk;
+    long file_off;
+    size_t bytes;
+    char *dst;
+};
+
+}  // namespace
+
+// worker w of W: the ranges w, w + W, ... through its own stream and two
+// pinned buffers (one piece read while the previous one is copied)
+static std::string upload_ranges(const std::vector<IcChunk> &chunks, const std::vector<Range> &ranges, int w,
+                                 int W, int device, size_t piece) {
     cudaError_t ce = cudaSetDevice(device);
     if (ce != cudaSuccess) return cudaGetErrorString(ce);
     cudaStream_t st = nullptr;
     char *buf[2] = {nullptr, nullptr};
     cudaEvent_t ev[2] = {nullptr, nullptr};
     bool used[2] = {false, false};
+    std::vector<int> fds(chunks.size(), -1);
     std::string err;
-    const int fd = open(ch.path.c_str(), O_RDONLY);
     auto cuda_ok = [&](cudaError_t e, const char *what) {
         if (e != cudaSuccess && err.empty()) err = std::string(what) + ": " + cudaGetErrorString(e);
         return e == cudaSuccess;
     };
-    if (fd < 0) err = " cannot read IC file !! " + ch.path;
-    if (err.empty() && cuda_ok(cudaStreamCreateWithFlags(&st, cudaStreamNonBlocking), "cudaStreamCreate")) {
+    if (cuda_ok(cudaStreamCreateWithFlags(&st, cudaStreamNonBlocking), "cudaStreamCreate")) {
         for (int k = 0; k < 2 && err.empty(); ++k) {
             cuda_ok(cudaHostAlloc(reinterpret_cast<void **>(&buf[k]), piece, cudaHostAllocDefault), "cudaHostAlloc");
             if (err.empty()) cuda_ok(cudaEventCreateWithFlags(&ev[k], cudaEventDisableTiming), "cudaEventCreate");
         }
     }
     int turn = 0;
-    // one block of the file -> device, through the two pinned buffers
-    auto stream_block = [&](long file_off, size_t nbytes, char *dst) {
-        for (size_t off = 0; off < nbytes && err.empty(); off += piece) {
+    for (size_t r = size_t(w); r < ranges.size() && err.empty(); r += size_t(W)) {
+        const Range &rg = ranges[r];
+        const IcChunk &ch = chunks[size_t(rg.chunk)];
+        if (fds[size_t(rg.chunk)] < 0) fds[size_t(rg.chunk)] = open(ch.path.c_str(), O_RDONLY);
+        const int fd = fds[size_t(rg.chunk)];
+        if (fd < 0) {
+            err = " cannot read IC file !! " + ch.path;
+            break;
+        }
+        for (size_t off = 0; off < rg.bytes && err.empty(); off += piece) {
             const int k = turn++ & 1;
-            const size_t len = std::min(piece, nbytes - off);
-            if (used[k] && !cuda_ok(cudaEventSynchronize(ev[k]), "cudaEventSynchronize")) return;
-            if (!pread_all(fd, buf[k], len, off_t(file_off + off))) {
+            const size_t len = std::min(piece, rg.bytes - off);
+            if (used[k] && !cuda_ok(cudaEventSynchronize(ev[k]), "cudaEventSynchronize")) break;
+            if (!pread_all(fd, buf[k], len, off_t(rg.file_off + long(off)))) {
                 err = "truncated Gadget blocks " + ch.path;
-                return;
+                break;
             }
-            if (!cuda_ok(cudaMemcpyAsync(dst + off, buf[k], len, cudaMemcpyHostToDevice, st), "cudaMemcpyAsync")) return;
+            if (!cuda_ok(cudaMemcpyAsync(rg.dst + off, buf[k], len, cudaMemcpyHostToDevice, st), "cudaMemcpyAsync"))
+                break;
             cuda_ok(cudaEventRecord(ev[k], st), "cudaEventRecord");
             used[k] = true;
         }
-    };
-    const long body = ch.base + (ref1 ? ch.lg : 0);
-    if (err.empty()) stream_block(pos_offset(), size_t(12 * ch.n), reinterpret_cast<char *>(d_pos + 3 * body));
-    if (err.empty()) stream_block(vel_offset(ch.n), size_t(12 * ch.n), reinterpret_cast<char *>(d_vel + 3 * body));
-    if (err.empty() && ref1) {
-        const size_t gb = size_t(12 * ch.lg);
-        const long tail = body + ch.n - ch.lg;
-        if (gb) {
-            cuda_ok(cudaMemcpyAsync(d_pos + 3 * ch.base, d_pos + 3 * tail, gb, cudaMemcpyDeviceToDevice, st), "ghosts");
-            cuda_ok(cudaMemcpyAsync(d_vel + 3 * ch.base, d_vel + 3 * tail, gb, cudaMemcpyDeviceToDevice, st), "ghosts");
-        }
-        cuda_ok(cudaMemsetAsync(d_pos + 3 * (body + ch.n), 0, 12, st), "cudaMemsetAsync");
-        cuda_ok(cudaMemsetAsync(d_vel + 3 * (body + ch.n), 0, 12, st), "cudaMemsetAsync");
     }
     if (st) cuda_ok(cudaStreamSynchronize(st), "cudaStreamSynchronize");
     for (int k = 0; k < 2; ++k) {
@@ -147,20 +156,55 @@ static std::string upload_chunk(const IcChunk &ch, bool ref1, float *d_pos, floa
         if (ev[k]) cudaEventDestroy(ev[k]);
     }
     if (st) cudaStreamDestroy(st);
-    if (fd >= 0) close(fd);
+    for (int fd : fds)
+        if (fd >= 0) close(fd);
     return err;
 }
 
 std::string ic_upload(const std::vector<IcChunk> &chunks, bool ref1, float *d_pos, float *d_vel, int device,
                       size_t piece_bytes) {
-    std::vector<std::string> errs(chunks.size());
+    // every block cut into ranges of a few pieces, spread over the workers
+    const size_t span = 4 * piece_bytes;
+    std::vector<Range> ranges;
+    for (size_t c = 0; c < chunks.size(); ++c) {
+        const IcChunk &ch = chunks[c];
+        const long body = ch.base + (ref1 ? ch.lg : 0);
+        const size_t bytes = size_t(12 * ch.n);
+        char *dpos = reinterpret_cast<char *>(d_pos + 3 * body), *dvel = reinterpret_cast<char *>(d_vel + 3 * body);
+        for (size_t off = 0; off < bytes; off += span) {
+            const size_t len = std::min(span, bytes - off);
+            ranges.push_back({int(c), pos_offset() + long(off), len, dpos + off});
+            ranges.push_back({int(c), vel_offset(ch.n) + long(off), len, dvel + off});
+        }
+    }
+    const int hw = int(std::thread::hardware_concurrency());
+    const int W = int(std::max<size_t>(1, std::min<size_t>(ranges.size(), size_t(std::min(16, std::max(1, hw))))));
+    std::vector<std::string> errs(static_cast<size_t>(W));
     std::vector<std::thread> pool;
-    for (size_t c = 0; c < chunks.size(); ++c)
-        pool.emplace_back([&, c] { errs[c] = upload_chunk(chunks[c], ref1, d_pos, d_vel, device, piece_bytes); });
+    for (int w = 0; w < W; ++w)
+        pool.emplace_back([&, w] { errs[size_t(w)] = upload_ranges(chunks, ranges, w, W, device, piece_bytes); });
     for (auto &t : pool) t.join();
     for (auto &e : errs)
         if (!e.empty()) return e;
-    return "";
+    if (!ref1) return "";
+    // ghosts (a device copy of each chunk's tail, in front of it) and the zero particle after it
+    cudaStream_t st = nullptr;
+    cudaError_t ce = cudaStreamCreateWithFlags(&st, cudaStreamNonBlocking);
+    for (size_t c = 0; c < chunks.size() && ce == cudaSuccess; ++c) {
+        const IcChunk &ch = chunks[c];
+        const long body = ch.base + ch.lg, tail = body + ch.n - ch.lg;
+        const size_t gb = size_t(12 * ch.lg);
+        if (gb) {
+            ce = cudaMemcpyAsync(d_pos + 3 * ch.base, d_pos + 3 * tail, gb, cudaMemcpyDeviceToDevice, st);
+            if (ce == cudaSuccess)
+                ce = cudaMemcpyAsync(d_vel + 3 * ch.base, d_vel + 3 * tail, gb, cudaMemcpyDeviceToDevice, st);
+        }
+        if (ce == cudaSuccess) ce = cudaMemsetAsync(d_pos + 3 * (body + ch.n), 0, 12, st);
+        if (ce == cudaSuccess) ce = cudaMemsetAsync(d_vel + 3 * (body + ch.n), 0, 12, st);
+    }
+    if (ce == cudaSuccess) ce = cudaStreamSynchronize(st);
+    if (st) cudaStreamDestroy(st);
+    return ce == cudaSuccess ? "" : std::string("IC ghost copies: ") + cudaGetErrorString(ce);
 }
 
 }  // namespace ifdm

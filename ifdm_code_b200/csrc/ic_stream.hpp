@@ -1,12 +1,12 @@
 // ic_stream.hpp -- Gadget chunk files streamed to the device.
 //
 // The reference reads each chunk whole into host vectors
-// (src/gadget_IC.h:259-353), then distributes the particles over the ranks
-// (:412-545).  Here the four chunks are read side by side, one thread per
-// chunk, in pieces through two pinned buffers per thread: while one piece is
-// copied to the device (asynchronous, on the thread's own stream) the next is
-// read.  Particles land directly at their place in the device arrays, in the
-// order the one-rank reference processes them:
+// (:412-545).  Here every position and velocity block is cut into byte
+// ranges that up to 16 threads read side by side, each in pieces through two
+// pinned buffers: while one piece is copied to the device (asynchronous, on
+// the thread's own stream) the next is read.  Particles land directly at
+// their place in the device arrays, in the order the one-rank reference
+// processes them:
 //
 //   per chunk c:  [ghosts: its last lg_c particles] [its n_c particles] [one zero particle]
 //
@@ -40,8 +40,9 @@ std::string ic_scan_chunks(const std::string &icpath, int nchunks, int N, bool r
                            long *np_total);
 
 // Fills d_pos / d_vel (3 floats per particle slot) from the files.  Returns
-// when the copies are complete.  piece_bytes: the size of one read.
+// when the copies are complete.  piece_bytes: the size of one read (each
+// worker pins two of them).
 std::string ic_upload(const std::vector<IcChunk> &chunks, bool ref1, float *d_pos, float *d_vel, int device,
-                      size_t piece_bytes = size_t(32) << 20);
+                      size_t piece_bytes = size_t(8) << 20);
 
 }  // namespace ifdm

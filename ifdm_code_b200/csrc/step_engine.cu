@@ -15,8 +15,18 @@
 #include <cstring>
 #include <type_traits>
 #include <algorithm>
+#include <mutex>
+#include <set>
 
 namespace ifdm {
+
+// guards this file's process-wide caches (kernel attributes per device, the
+// twiddle tables, the tensor-map encoder): contexts may be driven from
+// several host threads at once (the batched adjoint does)
+static std::mutex &setup_mutex() {
+    static std::mutex m;
+    return m;
+}
 
 const char *const kPassNames[kNumPasses] = {
     "T_timestep", "P1_kick_fft_z", "P2_fft_y", "P3_fft_x_drift_ifft_x", "P4_ifft_y",
@@ -60,8 +70,13 @@ template <typename R_, typename K_, int N> struct Box {
     }
 
     static std::string configure() {
-        static bool done = false;
-        if (done) return "";
+        // once per device (kernel attributes are per device), under the lock
+        // that guards every process-wide cache of this file
+        std::lock_guard<std::mutex> lk(setup_mutex());
+        static std::set<int> done_on;
+        int dev = 0;
+        CUDA_TRY(cudaGetDevice(&dev));
+        if (done_on.count(dev)) return "";
         CUDA_TRY(prep(k_kick_fft_z<R, K, N>, SMZ));
         CUDA_TRY(prep(k_fft_yx<R, K, N, -1, 1>, SM));
         CUDA_TRY(prep(k_fft_yx<R, K, N, +1, 1>, SM));
@@ -75,8 +90,7 @@ template <typename R_, typename K_, int N> struct Box {
         CUDA_TRY(prep(k_fft_z<R, K, N, -1>, SMZ));
         CUDA_TRY(prep(k_fft_z<R, K, N, +1>, SMZ));
         CUDA_TRY(prep(k_source_r2c_z<R, K, N>, SMZ));
-        int dev = 0, sms = 0;
-        CUDA_TRY(cudaGetDevice(&dev));
+        int sms = 0;
         CUDA_TRY(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));
         if constexpr (kZPipe) {
             using ZP = ZPipe<R, N>;
@@ -97,7 +111,7 @@ template <typename R_, typename K_, int N> struct Box {
             ygrid = sms * (by > 0 ? by : 1);
             xgrid = sms * (bx > 0 ? bx : 1);
         }
-        done = true;
+        done_on.insert(dev);
         return "";
     }
 
@@ -230,10 +244,16 @@ template <typename F> static std::string with_box2(int n, int prec, F &&f) {
 static std::string encode_map(CUtensorMap *m, void *base, bool f64, int rank, const cuuint64_t *dims,
                               const cuuint64_t *strides, const cuuint32_t *box) {
     static PFN_cuTensorMapEncodeTiled_v12000 fn = nullptr;
-    if (!fn) {
-        cudaDriverEntryPointQueryResult q;
-        CUDA_TRY(cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", (void **)&fn, cudaEnableDefault, &q));
-        if (q != cudaDriverEntryPointSuccess || !fn) return "cuTensorMapEncodeTiled unavailable";
+    {
+        std::lock_guard<std::mutex> lk(setup_mutex());
+        if (!fn) {
+            cudaDriverEntryPointQueryResult q;
+            CUDA_TRY(cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", (void **)&fn, cudaEnableDefault, &q));
+            if (q != cudaDriverEntryPointSuccess || !fn) {
+                fn = nullptr;
+                return "cuTensorMapEncodeTiled unavailable";
+            }
+        }
     }
     cuuint32_t estr[3] = {1, 1, 1};
     CUresult r = fn(m, f64 ? CU_TENSOR_MAP_DATA_TYPE_FLOAT64 : CU_TENSOR_MAP_DATA_TYPE_FLOAT32, (cuuint32_t)rank,
@@ -286,6 +306,7 @@ template <typename C> static std::vector<C> twiddles(int n) {
 // cached per-(n, precision) tables on the current device
 static std::string get_twiddles(int n, int prec, void **out) {
     struct Entry { int dev, n, prec; void *p; };
+    std::lock_guard<std::mutex> lk(setup_mutex());
     static std::vector<Entry> cache;
     int dev = 0;
     CUDA_TRY(cudaGetDevice(&dev));

@@ -292,17 +292,23 @@ template <typename R, typename K, int N, class P> struct BatchOps {
         fft_tile<C, M, TZ::EHD, +1, TZ::L, TZ::LP>(sm, twh);
         const K *smr = reinterpret_cast<const K *>(sm);
         constexpr KSplit<K> inv(1.0 / ((double)N * N * N));
-        double mx = 0.0;
+        // the scan window as one limit per tile, the running max on the pipe
+        // the pass leaves idle (as in the one-box c2r pass)
+        R *out = phi + row0 * N;
+        const bool inside = (long)(row0 + TZ::L) <= bx.win_rows;
+        const int lim =
+            inside ? TZ::L * N : (int)max(0L, min((long)TZ::L * N, (bx.win_rows - (long)row0) * N + bx.win_tail));
+        using MX = std::conditional_t<sizeof(K) == 4, double, R>;
+        MX mx = MX(0);
         for (int f = threadIdx.x; f < TZ::L * N; f += TZ::NT) {
             const int l = f / N, n = f % N;
             const R v = Cvt<R, K>::outr(mulk(smr[2 * ((n >> 1) * TZ::LP + l) + (n & 1)], inv.hi, inv.lo), salt,
                                         row0 * N + f);
-            phi[row0 * N + f] = v;
-            const long row = (long)(row0 + l);
-            if (row < bx.win_rows || (row == bx.win_rows && n < bx.win_tail)) mx = fmax(mx, (double)fabs(v));
+            out[f] = v;
+            if (f < lim) mx = fmax(mx, (MX)fabs(v));
         }
-        mx = warp_max(mx);
-        if ((threadIdx.x & 31) == 0) atomic_max_nonneg(&ts->maxphi_bits, mx);
+        const double m = warp_max((double)mx);
+        if ((threadIdx.x & 31) == 0) atomic_max_nonneg(&ts->maxphi_bits, m);
     }
 
     // one phase of one tile, chosen at compile time

@@ -28,10 +28,14 @@ template <typename R, typename K, int N, int AXIS = 1> struct TmaTile {
     using G = cx<R>;
     using C = cx<K>;
     static constexpr bool SPLIT = !std::is_same<R, K>::value;
-    // lines per tile: 128-byte rows, except for the FP32 x passes at N = 512,
-    // whose two chained transforms with compensated twiddles spill heavily at
-    // the 64-register cap of 1024 threads; 8 lines (512 threads) do not spill
-    static constexpr bool NARROW = !SPLIT && AXIS == 2 && sizeof(G) == 8 && N >= 512;
+    // lines per tile: 128-byte rows, except for FP32 at N = 512: the x
+    // passes' two chained transforms with compensated twiddles spill heavily
+    // at the 64-register cap of 1024 threads, so they take 8 lines (512
+    // threads, one block per SM); the y passes take 8 lines too, capped at 64
+    // registers so that two blocks share an SM (measured: P2/P4 0.531 ->
+    // 0.49 ms, P6/P8 0.30 -> 0.27 ms against 16 lines, one block per SM)
+    static constexpr bool NARROW = !SPLIT && sizeof(G) == 8 && N >= 512;
+    static constexpr int MINB = (NARROW && AXIS == 1) ? 2 : 1;  // resident blocks the registers must allow
     static constexpr int L = (SPLIT || NARROW) ? 8 : 128 / (int)sizeof(G);
     static constexpr int E = Plan<N>::E;
     static constexpr int T = N / E;
@@ -52,7 +56,7 @@ template <typename R, typename K, int N, int AXIS = 1> struct TmaTile {
 };
 
 template <typename R, typename K, int N, int AXIS, int MODE, int DIR>
-__global__ void __launch_bounds__(TmaTile<R, K, N, AXIS>::NT, 1)
+__global__ void __launch_bounds__(TmaTile<R, K, N, AXIS>::NT, TmaTile<R, K, N, AXIS>::MINB)
     k_yx_tma(const __grid_constant__ CUtensorMap map, cx<R> *__restrict__ data, int W, int VW, int ntiles,
              TState *__restrict__ ts, int pass, const cx<K> *__restrict__ drift, const cx<K> *__restrict__ tw) {
     using TL = TmaTile<R, K, N, AXIS>;

@@ -13,6 +13,9 @@
 
 namespace ifdm {
 
+// The tile of the y/x passes (16 FP32 lines, 1024 threads, one block per SM).
+// Half the lines under a 64-register cap (two blocks per SM, as the FP32 y
+// passes use) spilled and measured slower at 512^3: 1.03 -> 1.46 ms.
 template <typename R, int N> struct ZPipe {
     using TL = Tile<R, R, N>;
     using C = cx<R>;

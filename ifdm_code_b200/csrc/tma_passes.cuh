@@ -33,7 +33,9 @@ template <typename R, typename K, int N, int AXIS = 1> struct TmaTile {
     // at the 64-register cap of 1024 threads, so they take 8 lines (512
     // threads, one block per SM); the y passes take 8 lines too, capped at 64
     // registers so that two blocks share an SM (measured: P2/P4 0.531 ->
-    // 0.49 ms, P6/P8 0.30 -> 0.27 ms against 16 lines, one block per SM)
+    // 0.49 ms, P6/P8 0.30 -> 0.27 ms against 16 lines, one block per SM).
+    // 4-line x tiles, two blocks per SM at the same 128 registers (32-byte
+    // TMA rows), measured slower: P3 0.92 -> 1.31 ms, P7 0.52 -> 0.59 ms.
     static constexpr bool NARROW = !SPLIT && sizeof(G) == 8 && N >= 512;
     static constexpr int MINB = (NARROW && AXIS == 1) ? 2 : 1;  // resident blocks the registers must allow
     static constexpr int L = (SPLIT || NARROW) ? 8 : 128 / (int)sizeof(G);

@@ -37,8 +37,13 @@ template <typename R, typename K, int N, int AXIS = 1> struct TmaTile {
     // 4-line x tiles, two blocks per SM at the same 128 registers (32-byte
     // TMA rows), measured slower: P3 0.92 -> 1.31 ms, P7 0.52 -> 0.59 ms.
     static constexpr bool NARROW = !SPLIT && sizeof(G) == 8 && N >= 512;
-    static constexpr int MINB = (NARROW && AXIS == 1) ? 2 : 1;  // resident blocks the registers must allow
-    static constexpr int L = (SPLIT || NARROW) ? 8 : 128 / (int)sizeof(G);
+    // FP64 y passes at N = 512: 4 lines (64-byte rows, 256 threads) so that
+    // two blocks share an SM at the same 128 registers (measured: P2/P4
+    // 0.89 -> 0.85 ms, P6/P8 0.50 -> 0.45 ms)
+    static constexpr bool NARROW64 = !SPLIT && sizeof(G) == 16 && AXIS == 1 && N >= 512;
+    static constexpr int MINB = ((NARROW && AXIS == 1) || NARROW64) ? 2 : 1;  // resident blocks the registers must allow
+    static constexpr int L = NARROW64 ? 4 : (SPLIT || NARROW) ? 8 : 128 / (int)sizeof(G);
+    static constexpr bool SWZ = NARROW || NARROW64;  // slot swizzle of the exchange tile
     static constexpr int E = Plan<N>::E;
     static constexpr int T = N / E;
     static constexpr int NT = L * T;
@@ -120,7 +125,7 @@ __global__ void __launch_bounds__(TmaTile<R, K, N, AXIS>::NT, TmaTile<R, K, N, A
         stage_load<C, N, E, L, L, R0>(land, v, l, t);
         if constexpr (TL::OWN_WORK) fence_proxy_async_smem();  // slot is released at the next barrier
         stage_compute<C, N, E, (MODE == 0 ? DIR : -1), R0, 1>(v, tw, t);
-        RegChain<C, N, E, (MODE == 0 ? DIR : -1), L, LPW, 1, R0, TL::NARROW>::run(wk, v, tw, l, t, true);
+        RegChain<C, N, E, (MODE == 0 ? DIR : -1), L, LPW, 1, R0, TL::SWZ>::run(wk, v, tw, l, t, true);
         if (MODE != 0) {
             // v[b*RL + r] holds element n = (t + T*b) + r*N/RL of the forward transform
             if (MODE == 1) {
@@ -153,7 +158,7 @@ __global__ void __launch_bounds__(TmaTile<R, K, N, AXIS>::NT, TmaTile<R, K, N, A
                         v[b * RL + r] = cscale(v[b * RL + r], k2 == 0 ? K(0) : K(-1) / K(k2));
                     }
             }
-            fft_regs_chained<C, N, E, +1, L, LPW, TL::NARROW>(wk, v, tw, l, t, true);
+            fft_regs_chained<C, N, E, +1, L, LPW, TL::SWZ>(wk, v, tw, l, t, true);
         }
         if ((g % W) < VW) {
             const size_t b0 = AXIS == 1 ? size_t(g / W) * N * W + size_t(g % W) : size_t(g);

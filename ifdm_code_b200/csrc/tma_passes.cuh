@@ -39,7 +39,8 @@ template <typename R, typename K, int N, int AXIS = 1> struct TmaTile {
     static constexpr bool NARROW = !SPLIT && sizeof(G) == 8 && N >= 512;
     // FP64 y passes at N = 512: 4 lines (64-byte rows, 256 threads) so that
     // two blocks share an SM at the same 128 registers (measured: P2/P4
-    // 0.89 -> 0.85 ms, P6/P8 0.50 -> 0.45 ms)
+    // 0.89 -> 0.85 ms, P6/P8 0.50 -> 0.45 ms; the FP64 x passes measured
+    // slower that way: P3 1.39 -> 1.93 ms, P7 0.71 -> 0.78 ms)
     static constexpr bool NARROW64 = !SPLIT && sizeof(G) == 16 && AXIS == 1 && N >= 512;
     static constexpr int MINB = ((NARROW && AXIS == 1) || NARROW64) ? 2 : 1;  // resident blocks the registers must allow
     static constexpr int L = NARROW64 ? 4 : (SPLIT || NARROW) ? 8 : 128 / (int)sizeof(G);

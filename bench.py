@@ -446,12 +446,21 @@ def run_ours(args):
     for prec in ("fp64", "mixed", "fp32"):
         sim = ifdm.Simulation(MFDM, G, XMAX, N, precision=prec, device=local)
         sim.set_psi(psi0, A0)
+        t_w = time.perf_counter()
         sim.step(W, C)
         sim.synchronize()
+        per_step = (time.perf_counter() - t_w) / max(W, 1)
+        # the clock record spans at least ~1.2 s of the same load: untimed steps
+        # of this box before and after the timed ones keep the GPU busy while
+        # nvidia-smi samples (the timed region alone may be 0.1 s)
+        pad = max(1, min(400, int(0.6 / max(per_step, 1e-4))))
         barrier()
         clk = ClockSampler(local)
         with clk:
+            sim.step(pad, C)
             ms = time_steps(sim, K, 0, C, torch)
+            sim.step(pad, C)
+            sim.synchronize()
         barrier()
         ms = max_over_ranks(ms)
         prof = sim.profile_passes(max(3, min(10, K)), C)
@@ -539,6 +548,16 @@ def run_ours(args):
 
     # the 256^3, g = 0 precision config (1000 steps), reported beside the headline
     prec256 = precision_report(256, 0.0, 1000, local) if (args.precision_steps > 0 and N == 512) else None
+    # the 256^3 precision config with the self-interaction strength the 512^3
+    # configuration names (0.1 rad per step at the densest cell), at which the
+    # scheme is stable at 256^3
+    prec256g = None
+    if args.precision_steps > 0 and N == 512:
+        from ifdm_code_b200.synthetic_ic import zeldovich_psi as _zp
+        C256 = dt_scale_for(256)
+        g256 = g_for_phase(256, _zp(256, xmax=XMAX, seed=0, a=A0, mfdm=MFDM), C256, 0.1)
+        prec256g = precision_report(256, g256, 1000, local)
+        prec256g["g_phase_rad"] = 0.1
 
     batch = {p: run_batch(args, p, local, args.adjoint_steps if p == head else 0)
              for p in dict.fromkeys([head, "mixed"])} if args.batch_steps > 0 else None
@@ -610,6 +629,7 @@ def run_ours(args):
                       "roofline": roofline(res[p], p), "clocks": res[p]["clocks"]} for p in res},
         "precision": prec_report,
         "precision_256_g0": prec256,
+        "precision_256_g01": prec256g,
         "cufft_reference": fft_ref,
         "adjoint": adj,
         "batch": batch,
@@ -788,6 +808,35 @@ def run_reference(args):
     }))
 
 
+def run_stability(args):
+    """FP64 record of the split-step scheme's stability at N^3 under the
+    self-interaction strengths 0.1, 0.03 and 0.01 rad per step at the densest
+    cell (the benchmark's fixed-step schedule): max|psi|^2 relative to its
+    initial value, a and the limiting criterion every 10 steps."""
+    import ifdm_code_b200 as ifdm
+    from ifdm_code_b200.synthetic_ic import zeldovich_psi
+
+    N = args.res
+    C = dt_scale_for(N)
+    psi0 = zeldovich_psi(N, xmax=XMAX, seed=0, a=A0, mfdm=MFDM)
+    out = {"res": N, "dt_scale": C, "steps": args.precision_steps, "every": 10, "runs": {}}
+    for phase in (0.1, 0.03, 0.01):
+        G = g_for_phase(N, psi0, C, phase)
+        trace = []
+        with ifdm.Simulation(MFDM, G, XMAX, N) as sim:
+            sim.set_psi(psi0, A0)
+            sim.step(1, C)
+            r0 = sim.state()["max_rho"]
+            for n in range(1, args.precision_steps, 10):
+                st = sim.state()
+                trace.append([int(st["steps"]), round(st["max_rho"] / r0, 4), round(st["a"], 6), int(st["criterion"])])
+                sim.step(min(10, args.precision_steps - n), C)
+            st = sim.state()
+            trace.append([int(st["steps"]), round(st["max_rho"] / r0, 4), round(st["a"], 6), int(st["criterion"])])
+        out["runs"][str(phase)] = {"g_eV_cm3": G, "trace": trace}
+    print(json.dumps(out))
+
+
 def run_profile(args):
     """Short fixed run of one precision for ncu captures: W + K steps, no timing."""
     import ifdm_code_b200 as ifdm
@@ -815,6 +864,8 @@ def main():
     ap.add_argument("--profile", action="store_true", help="plain W+K steps of --precision (for ncu)")
     ap.add_argument("--profile-ic", action="store_true", help="only the IC section at --ic-res (for ncu)")
     ap.add_argument("--calibrate-g", action="store_true", help="print the g of the self-interaction config")
+    ap.add_argument("--stability", action="store_true",
+                    help="FP64 max|psi|^2 trace at --res under 0.1/0.03/0.01 rad per step (no timing)")
     ap.add_argument("--precision", choices=["fp32", "fp64", "mixed"], default="mixed")
     ap.add_argument("--adjoint-steps", type=int, default=40, help="steps of the adjoint timing (0 skips it)")
     ap.add_argument("--g-phase", type=float, default=0.01,
@@ -840,6 +891,8 @@ def main():
         import ifdm_code_b200 as ifdm
 
         print(json.dumps(ic_section(ifdm, args.ic_res, 0, 0)))
+    elif args.stability:
+        run_stability(args)
     elif args.calibrate_g:
         calibrate_g(args)
     elif args.impl == "reference":

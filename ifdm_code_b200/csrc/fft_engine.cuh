@@ -254,17 +254,19 @@ __device__ __forceinline__ void fft_tile(C *sm, const C *__restrict__ tw) {
 // The same Stockham stages with the stage inputs held in registers v[E]:
 // v[b*RAD + r] is element j + r*N/RAD of line l, j = t + T*b.
 //
-// SW: element n of a line sits in slot n ^ ((n >> 3) & 1) of the exchange
-// tile.  With 8 unpadded float2 lines (the narrow FP32 x tiles) the first
-// radix-8 stage stores element 8j + r of lines l = 0..7 for two consecutive j
-// in one half-warp, and both land in the same banks (2-way conflicts on every
-// such store); swapping odd and even slots where bit 3 is set moves one of the
-// two to the other half of the banks, and the other store and load patterns
-// of the 8 x 8 x 8 chain stay conflict-free (measured at 512^3: P3
-// 0.936 -> 0.917 ms, P7 0.521 -> 0.519 ms).
-template <bool SW> __device__ __forceinline__ int slot(int n) { return SW ? (n ^ ((n >> 3) & 1)) : n; }
+// SW: element n of a line sits in slot n ^ ((n >> 3) & SW) of the exchange
+// tile (SW = 0: no swizzle).  With 8 unpadded float2 lines (the narrow FP32
+// x tiles) the first radix-8 stage stores element 8j + r of lines l = 0..7
+// for two consecutive j in one half-warp, and both land in the same banks
+// (2-way conflicts on every such store); SW = 1 swaps odd and even slots where
+// bit 3 is set, which moves one of the two to the other half of the banks,
+// and the other store and load patterns of the 8 x 8 x 8 chain stay
+// conflict-free (measured at 512^3: P3 0.936 -> 0.917 ms, P7 0.521 -> 0.519
+// ms).  With 4 lines a half-warp stores for four consecutive j (4-way); SW = 3
+// spreads them over four slots.
+template <int SW> __device__ __forceinline__ int slot(int n) { return SW ? (n ^ ((n >> 3) & SW)) : n; }
 
-template <typename C, int N, int E, int L, int LP, int RAD, typename SrcT, bool SW = false>
+template <typename C, int N, int E, int L, int LP, int RAD, typename SrcT, int SW = 0>
 __device__ __forceinline__ void stage_load(const SrcT *src, C *v, int l, int t) {
     constexpr int T = N / E, NB = E / RAD, STRIDE = N / RAD;
 #pragma unroll
@@ -290,7 +292,7 @@ __device__ __forceinline__ void stage_compute(C *v, const C *__restrict__ tw, in
     }
 }
 
-template <typename C, int N, int E, int L, int LP, int RAD, int NS, bool SW = false>
+template <typename C, int N, int E, int L, int LP, int RAD, int NS, int SW = 0>
 __device__ __forceinline__ void stage_store(C *dst, const C *v, int l, int t) {
     constexpr int T = N / E, NB = E / RAD;
 #pragma unroll
@@ -304,7 +306,7 @@ __device__ __forceinline__ void stage_store(C *dst, const C *v, int l, int t) {
 
 // Stages S.. of a transform whose stage S-1 outputs are in v: round trip
 // through `work` (barrier, store, barrier, load) then compute stage S.
-template <typename C, int N, int E, int DIR, int L, int LP, int S, int NS, bool SW = false>
+template <typename C, int N, int E, int DIR, int L, int LP, int S, int NS, int SW = 0>
 struct RegChain {
     __device__ __forceinline__ static void run(C *work, C *v, const C *__restrict__ tw, int l, int t, bool active) {
         if constexpr (S < Plan<N>::NST) {
@@ -338,7 +340,7 @@ __device__ __forceinline__ void fft_regs(const SrcT *src, C *work, C *v, const C
 
 // Second transform straight from the registers of a first one (requires the
 // plan's first and last radix to be equal).
-template <typename C, int N, int E, int DIR, int L, int LP, bool SW = false>
+template <typename C, int N, int E, int DIR, int L, int LP, int SW = 0>
 __device__ __forceinline__ void fft_regs_chained(C *work, C *v, const C *__restrict__ tw, int l, int t, bool active) {
     constexpr int R0 = Plan<N>::R[0];
     static_assert(Plan<N>::R[0] == Plan<N>::R[Plan<N>::NST - 1], "chained transform needs equal first/last radix");

@@ -187,11 +187,9 @@ static int psi_to_host(ifdm_ctx *c, double *host, int which) {
         CTX_CUDA(c, cudaStreamSynchronize(c->stream));
         return IFDM_OK;
     }
-    if (ensure_out(c)) return IFDM_ERR_CUDA;
-    if (c->snap.ready()) CTX_STR(c, IFDM_ERR_CUDA, c->snap.before_stage(c->stream));
-    CTX_STR(c, IFDM_ERR_CUDA, c->eng.psi_out(c->d_out, which));
-    CTX_CUDA(c, cudaMemcpyAsync(host, c->d_out, c->eng.n3() * 2 * sizeof(double), cudaMemcpyDeviceToHost, c->stream));
-    CTX_CUDA(c, cudaStreamSynchronize(c->stream));
+    // host buffer: chunked conversion and copy through the engine's own
+    // staging slots (the snapshot staging buffer is not touched)
+    CTX_STR(c, IFDM_ERR_CUDA, c->eng.psi_to_host(host, which));
     return IFDM_OK;
 }
 

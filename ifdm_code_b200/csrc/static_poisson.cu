@@ -11,7 +11,8 @@
 // Host code must not pass the array's name to a kernel: on the host that name
 // is only a stand-in for the device symbol.  The first call on each device
 // looks up the array's device address with cudaGetSymbolAddress while that
-// device is current and keeps it for later calls on that device.
+// device is current, and sets the shared-memory attributes of the kernels of
+// every supported size; later calls on that device reuse both.
 #include "../../include/ifdm.h"
 #include "physics.hpp"
 #include "step_kernels.cuh"
@@ -65,33 +66,6 @@ static int static_poisson_n(unsigned char *base, const double2 *psi, double *phi
     constexpr int NHP = half_pitch<double>(N);
     static_assert(kOffPart + 3 * sizeof(double) * (size_t(N) * N / TL::L) <= kOffTw, "partial sums must fit");
     if (static_bytes_needed<N>() > kStaticScratchBytes) return IFDM_ERR_UNSUPPORTED;
-    // kernels above 48 KB of shared memory need the attribute, once per device (no allocation)
-    static std::mutex attr_mu;
-    static bool attr_done[64] = {};
-    int dev = 0;
-    if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= 64) return IFDM_ERR_CUDA;
-    cudaError_t attr_err = cudaSuccess;
-    {
-        std::lock_guard<std::mutex> lock(attr_mu);
-        if (!attr_done[dev]) {
-        attr_err = cudaFuncSetAttribute(k_density_r2c_z<double, double, N, false>,
-                                        cudaFuncAttributeMaxDynamicSharedMemorySize, (int)TL::SMEM);
-        if (attr_err == cudaSuccess)
-            attr_err = cudaFuncSetAttribute(k_fft_yx<double, double, N, -1, 1>,
-                                            cudaFuncAttributeMaxDynamicSharedMemorySize, (int)TL::SMEM);
-        if (attr_err == cudaSuccess)
-            attr_err = cudaFuncSetAttribute(k_fft_yx<double, double, N, +1, 1>,
-                                            cudaFuncAttributeMaxDynamicSharedMemorySize, (int)TL::SMEM);
-        if (attr_err == cudaSuccess)
-            attr_err = cudaFuncSetAttribute(k_fft_x_poisson<double, double, N>,
-                                            cudaFuncAttributeMaxDynamicSharedMemorySize, (int)TL::SMEM);
-        if (attr_err == cudaSuccess)
-            attr_err = cudaFuncSetAttribute(k_c2r_z_phi<double, double, N>,
-                                            cudaFuncAttributeMaxDynamicSharedMemorySize, (int)TL::SMEM9);
-        if (attr_err != cudaSuccess) return IFDM_ERR_CUDA;
-        attr_done[dev] = true;
-        }
-    }
     TState *ts = reinterpret_cast<TState *>(base + kOffState);
     double *part = reinterpret_cast<double *>(base + kOffPart);
     double2 *tw = reinterpret_cast<double2 *>(base + kOffTw);
@@ -113,8 +87,30 @@ static int static_poisson_n(unsigned char *base, const double2 *psi, double *phi
     return cudaGetLastError() == cudaSuccess ? IFDM_OK : IFDM_ERR_CUDA;
 }
 
-// device address of g_static_scratch, looked up once per device
-static int static_scratch_address(unsigned char **out) {
+// kernels above 48 KB of shared memory need the attribute (no allocation)
+template <int N> static cudaError_t static_attributes() {
+    using TL = Tile<double, double, N>;
+    cudaError_t e = cudaFuncSetAttribute(k_density_r2c_z<double, double, N, false>,
+                                         cudaFuncAttributeMaxDynamicSharedMemorySize, (int)TL::SMEM);
+    if (e == cudaSuccess)
+        e = cudaFuncSetAttribute(k_fft_yx<double, double, N, -1, 1>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                 (int)TL::SMEM);
+    if (e == cudaSuccess)
+        e = cudaFuncSetAttribute(k_fft_yx<double, double, N, +1, 1>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                 (int)TL::SMEM);
+    if (e == cudaSuccess)
+        e = cudaFuncSetAttribute(k_fft_x_poisson<double, double, N>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                 (int)TL::SMEM);
+    if (e == cudaSuccess)
+        e = cudaFuncSetAttribute(k_c2r_z_phi<double, double, N>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                 (int)TL::SMEM9);
+    return e;
+}
+
+// Once per device, with that device current: the device address of
+// g_static_scratch and the kernel attributes of every supported size, so
+// that no later call on that device does any set-up work.
+static int static_setup(unsigned char **out) {
     constexpr int kMaxDevices = 64;
     static void *addr[kMaxDevices] = {};
     static std::mutex mu;
@@ -124,6 +120,9 @@ static int static_scratch_address(unsigned char **out) {
     if (!addr[dev]) {
         void *p = nullptr;
         if (cudaGetSymbolAddress(&p, g_static_scratch) != cudaSuccess || !p) return IFDM_ERR_CUDA;
+        if (static_attributes<16>() != cudaSuccess || static_attributes<32>() != cudaSuccess ||
+            static_attributes<48>() != cudaSuccess || static_attributes<64>() != cudaSuccess)
+            return IFDM_ERR_CUDA;
         addr[dev] = p;
     }
     *out = static_cast<unsigned char *>(addr[dev]);
@@ -134,10 +133,10 @@ static int static_scratch_address(unsigned char **out) {
 
 extern "C" int ifdm_poisson_static(const double *psi, double *phi, int res, double mfdm, double xmax, void *stream) {
     using namespace ifdm;
-    if (!psi || !phi || !(mfdm > 0) || !(xmax > 0)) return IFDM_ERR_ARGS;
+    if (!psi || !phi || res <= 0 || !(mfdm > 0) || !(xmax > 0)) return IFDM_ERR_ARGS;
     if (res > kStaticMaxRes) return IFDM_ERR_UNSUPPORTED;
     unsigned char *base = nullptr;
-    int rc = static_scratch_address(&base);
+    int rc = static_setup(&base);
     if (rc != IFDM_OK) return rc;
     // phi = 4 pi G m_solar (xmax/pi)^2 * (-F^-1[F[|psi|^2] / kappa^2] / N^3)
     const double ms = mfdm * phys::kg2eV / phys::kg2solar;

@@ -5,6 +5,7 @@
 #include "timestep.cuh"
 #include "tma_passes.cuh"
 #include "zpass_pipe.cuh"
+#include "zpass_tma.cuh"
 #include "adjoint_kernels.cuh"
 
 #include <cudaTypedefs.h>
@@ -99,6 +100,19 @@ template <typename R_, typename K_, int N> struct Box {
             CUDA_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&b5, k_density_r2c_z_pipe<R, N>, ZP::NT, ZP::SMEM5));
             zgrid = sms * (b5 > 0 ? b5 : 1);
         }
+        if constexpr (kZT) {
+            using Z = ZT<N>;
+            CUDA_TRY(prep(k_kick_fft_z_tma<N, ZST1, ZB1>, ZSM1));
+            CUDA_TRY(prep(k_density_r2c_z_tma<N, ZST5, ZB5>, ZSM5));
+            CUDA_TRY(prep(k_c2r_z_tma<N, ZST9, ZB9>, ZSM9));
+            int b1 = 0, b5 = 0, b9 = 0;
+            CUDA_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&b1, k_kick_fft_z_tma<N, ZST1, ZB1>, Z::NT, ZSM1));
+            CUDA_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&b5, k_density_r2c_z_tma<N, ZST5, ZB5>, Z::NT, ZSM5));
+            CUDA_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&b9, k_c2r_z_tma<N, ZST9, ZB9>, Z::NT, ZSM9));
+            zt1grid = sms * (b1 > 0 ? b1 : 1);
+            zt5grid = sms * (b5 > 0 ? b5 : 1);
+            zt9grid = sms * (b9 > 0 ? b9 : 1);
+        }
         if constexpr (kTma) {
             CUDA_TRY(prep(k_yx_tma<R, K, N, 1, 0, -1>, TT::SMEM));
             CUDA_TRY(prep(k_yx_tma<R, K, N, 1, 0, +1>, TT::SMEM));
@@ -121,6 +135,14 @@ template <typename R_, typename K_, int N> struct Box {
     // than three plain blocks), and pipelined P1/P9 gained nothing.
     static constexpr bool kTma = N >= 128;
     static constexpr bool kZPipe = N >= 128 && std::is_same<R, float>::value && std::is_same<K, float>::value;
+    // FP32 z passes fed by bulk copies (zpass_tma.cuh) for N >= 256; ring
+    // depth and resident blocks per SM of P1, P5 and P9
+    static constexpr bool kZT = N >= 256 && std::is_same<R, float>::value && std::is_same<K, float>::value;
+    static constexpr int ZST1 = 2, ZB1 = 2, ZST5 = 3, ZB5 = 2, ZST9 = 3, ZB9 = 2;
+    static constexpr size_t ZSM1 = kZT ? ZST1 * ZT<(kZT ? N : 256)>::SLOT1 + 64 : 0;
+    static constexpr size_t ZSM5 = kZT ? ZST5 * ZT<(kZT ? N : 256)>::SLOT5 + 64 : 0;
+    static constexpr size_t ZSM9 = kZT ? ZST9 * ZT<(kZT ? N : 256)>::SLOT9 + 64 : 0;
+    static inline int zt1grid = 0, zt5grid = 0, zt9grid = 0;  // persistent grids of the bulk-copy z passes
     using TT = TmaTile<R, K, N, 1>;
     using TX = TmaTile<R, K, N, 2>;
     static inline int zgrid = 0;             // persistent grid of the pipelined P5
@@ -140,6 +162,19 @@ template <typename R_, typename K_, int N> struct Box {
     static void pass(int p, cudaStream_t s, G *psi, R *phi, G *rhok, TState *ts, const C *drift, const C *tw,
                      const C *twh, long wr, int wt, const CUtensorMap *tm = nullptr) {
         const unsigned nt = TL::NT;
+        if constexpr (kZT) {
+            if (tm && (p == 1 || p == 5 || p == 9)) {
+                using Z = ZT<N>;
+                const int nz = int(size_t(N) * N / Z::L);
+                if (p == 1)
+                    k_kick_fft_z_tma<N, ZST1, ZB1><<<zt1grid, Z::NT, ZSM1, s>>>(psi, phi, ts, tw, nz);
+                else if (p == 5)
+                    k_density_r2c_z_tma<N, ZST5, ZB5><<<zt5grid, Z::NT, ZSM5, s>>>(psi, rhok, ts, tw, nz);
+                else
+                    k_c2r_z_tma<N, ZST9, ZB9><<<zt9grid, Z::NT, ZSM9, s>>>(rhok, phi, ts, wr, wt, tw, nz / 2);
+                return;
+            }
+        }
         if constexpr (kZPipe) {
             if (tm && p == 5 && std::getenv("IFDM_NO_ZPIPE") == nullptr) {
                 using ZP = ZPipe<R, N>;
@@ -348,6 +383,24 @@ StepEngine::~StepEngine() {
     cudaFree(ts_adj_);
     cudaFree(drift64_adj_);
     cudaFree(drift32_adj_);
+    if (copy_stream_) cudaStreamSynchronize(copy_stream_);
+    for (int s = 0; s < 2; ++s) {
+        cudaFree(stage_[s]);
+        if (ev_copied_[s]) cudaEventDestroy(ev_copied_[s]);
+        if (ev_free_[s]) cudaEventDestroy(ev_free_[s]);
+    }
+    if (copy_stream_) cudaStreamDestroy(copy_stream_);
+}
+
+std::string StepEngine::ensure_staging() {
+    if (stage_[0]) return "";
+    CUDA_TRY(cudaStreamCreateWithFlags(&copy_stream_, cudaStreamNonBlocking));
+    for (int s = 0; s < 2; ++s) {
+        CUDA_TRY(cudaMalloc(&stage_[s], kStageElems * sizeof(double2)));
+        CUDA_TRY(cudaEventCreateWithFlags(&ev_copied_[s], cudaEventDisableTiming));
+        CUDA_TRY(cudaEventCreateWithFlags(&ev_free_[s], cudaEventDisableTiming));
+    }
+    return "";
 }
 
 std::string StepEngine::init(const EngineConfig &cfg, cudaStream_t stream) {
@@ -440,22 +493,58 @@ std::string StepEngine::load_psi(const double *psi, bool on_device, double a, do
 
         CUDA_TRY(cudaGetLastError());
     } else {
-        const size_t chunk = std::min<size_t>(n3, size_t(1) << 22);
-        double2 *stage = nullptr;
-        CUDA_TRY(cudaMalloc(&stage, chunk * sizeof(double2)));
-        for (size_t off = 0; off < n3; off += chunk) {
-            const size_t cnt = std::min(chunk, n3 - off);
-            CUDA_TRY(cudaMemcpyAsync(stage, psi + 2 * off, cnt * sizeof(double2), cudaMemcpyHostToDevice, stream_));
+        // chunk i: host -> slot i%2 on the copy stream, then the conversion on
+        // the compute stream; the copy of chunk i+1 runs during conversion i,
+        // and a slot is refilled only after its previous conversion finished
+        std::string e2 = ensure_staging();
+        if (!e2.empty()) return e2;
+        int i = 0;
+        for (size_t off = 0; off < n3; off += kStageElems, ++i) {
+            const int s = i & 1;
+            const size_t cnt = std::min(kStageElems, n3 - off);
+            CUDA_TRY(cudaStreamWaitEvent(copy_stream_, ev_free_[s], 0));
+            CUDA_TRY(cudaMemcpyAsync(stage_[s], psi + 2 * off, cnt * sizeof(double2), cudaMemcpyHostToDevice,
+                                     copy_stream_));
+            CUDA_TRY(cudaEventRecord(ev_copied_[s], copy_stream_));
+            CUDA_TRY(cudaStreamWaitEvent(stream_, ev_copied_[s], 0));
             if (prec == 0)
-                k_psi_in<double><<<1184, 256, 0, stream_>>>(stage, (double2 *)psi_ + off, invS, cnt);
+                k_psi_in<double><<<1184, 256, 0, stream_>>>(stage_[s], (double2 *)psi_ + off, invS, cnt);
             else
-                k_psi_in<float><<<1184, 256, 0, stream_>>>(stage, (float2 *)psi_ + off, invS, cnt);
+                k_psi_in<float><<<1184, 256, 0, stream_>>>(stage_[s], (float2 *)psi_ + off, invS, cnt);
             CUDA_TRY(cudaGetLastError());
+            CUDA_TRY(cudaEventRecord(ev_free_[s], stream_));
         }
-        CUDA_TRY(cudaStreamSynchronize(stream_));
-        cudaFree(stage);
+        // the caller may reuse its buffer once every copy has landed
+        CUDA_TRY(cudaStreamSynchronize(copy_stream_));
     }
     return launch_initial_density();
+}
+
+std::string StepEngine::psi_to_host(double *host_out, int which) {
+    std::string e = ensure_staging();
+    if (!e.empty()) return e;
+    const size_t n3 = n3_();
+    int i = 0;
+    for (size_t off = 0; off < n3; off += kStageElems, ++i) {
+        const int s = i & 1;
+        const size_t cnt = std::min(kStageElems, n3 - off);
+        // slot s is rewritten only after its previous copy to the host finished
+        CUDA_TRY(cudaStreamWaitEvent(stream_, ev_free_[s], 0));
+        if (cfg_.precision == 0)
+            k_psi_out<double><<<1184, 256, 0, stream_>>>((const double2 *)psi_ + off, (const double *)phi_ + off, ts_,
+                                                         which, S_, stage_[s], cnt);
+        else
+            k_psi_out<float><<<1184, 256, 0, stream_>>>((const float2 *)psi_ + off, (const float *)phi_ + off, ts_,
+                                                        which, S_, stage_[s], cnt);
+        CUDA_TRY(cudaGetLastError());
+        CUDA_TRY(cudaEventRecord(ev_copied_[s], stream_));
+        CUDA_TRY(cudaStreamWaitEvent(copy_stream_, ev_copied_[s], 0));
+        CUDA_TRY(cudaMemcpyAsync(host_out + 2 * off, stage_[s], cnt * sizeof(double2), cudaMemcpyDeviceToHost,
+                                 copy_stream_));
+        CUDA_TRY(cudaEventRecord(ev_free_[s], copy_stream_));
+    }
+    CUDA_TRY(cudaStreamSynchronize(copy_stream_));
+    return "";
 }
 
 std::string StepEngine::launch_initial_density() {

@@ -57,6 +57,11 @@ class StepEngine {
     std::vector<double> pass_bytes() const;
     // psi as complex128 into dev_out (device), which: 0 raw, 1 snapshot kick, 2 pending kick.
     std::string psi_out(double *dev_out, int which);
+    // psi as complex128 into a host buffer (pinned for full speed): chunks
+    // converted on the compute stream and copied on the copy stream through
+    // the two staging slots, each copy overlapping the next conversion.
+    // Returns once the host buffer holds the whole field.
+    std::string psi_to_host(double *host_out, int which);
     std::string phi_out(double *dev_out);
     // copy the TState to host (synchronous)
     std::string read_state(TState &out);
@@ -88,7 +93,16 @@ class StepEngine {
     std::string launch_passes(cudaEvent_t *ev);  // ev: optional 10 events (after each pass)
     std::string launch_initial_density();
     std::string set_physics(double a, double rhoc);
+    std::string ensure_staging();
     size_t n3_() const;
+
+    // host transfers: two device slots of kStageElems complex128 each, a copy
+    // stream, and per slot an event "copy done" and "slot free" (allocated on
+    // the first host transfer, kept for the context's lifetime)
+    static constexpr size_t kStageElems = size_t(1) << 22;
+    double2 *stage_[2] = {nullptr, nullptr};
+    cudaStream_t copy_stream_ = nullptr;
+    cudaEvent_t ev_copied_[2] = {nullptr, nullptr}, ev_free_[2] = {nullptr, nullptr};
 
     EngineConfig cfg_{};
     cudaStream_t stream_ = nullptr;

@@ -1,0 +1,306 @@
+// zpass_tma.cuh -- persistent z passes fed by bulk copies (FP32, N >= 256).
+//
+// The z passes work on whole rows (z fastest), which are contiguous in HBM.
+// Each CTA keeps a ring of ST slots; thread 0 keeps ST-1 tiles of rows in
+// flight with one untiled cp.async.bulk per row (completion on one mbarrier
+// per slot), so the bytes in flight no longer depend on registers, while the
+// CTA transforms the current tile with the register-resident Stockham chain
+// of the y/x passes.  Rows land at a pitch padded by 16 bytes: the first
+// stage reads element n of row l with the row index fastest across a warp,
+// and the pad puts those rows in different banks.  Later stages exchange
+// through the same slot laid out [n][l] (the swizzled 8-line tile of the
+// narrow x passes).  Every mbarrier wait is bounded (error bit in TState).
+//
+//   k_kick_fft_z_tma      P1: kick with the merged coefficients, remove the
+//                         offset c, forward FFT along z.
+//   k_density_r2c_z_tma   P5: inverse FFT along z, add c -> psi, density
+//                         rho = |psi|^2 - mu, max |psi|^2, and the real-to-
+//                         half-complex FFT of rho: rows l and l+4 of the tile
+//                         packed as one complex line rho_l + i rho_{l+4},
+//                         one N-point complex FFT, then
+//                         X_l = (Z_k + conj Z_{N-k})/2,
+//                         X_{l+4} = -i (Z_k - conj Z_{N-k})/2   (k = 0..N/2).
+//   k_c2r_z_tma           P9: the inverse of that packing: half rows l and
+//                         l+8 of a 16-row tile become Z = X_l + i X_{l+8}
+//                         on the full circle (X_{N-k} = conj X_k), one
+//                         N-point inverse FFT gives N phi_l + i N phi_{l+8};
+//                         scale by 1/N^3, store, max|phi| over the
+//                         reference's scan window.
+// The packed transforms need no post-twiddle (the half-length method of
+// k_density_r2c_z / k_c2r_z_phi does): the same N-point plan and table as
+// the complex passes.
+#pragma once
+
+#include "step_kernels.cuh"
+#include "tma.cuh"
+
+namespace ifdm {
+
+// Tile geometry of the FP32 z passes: 8 complex lines per tile (NT threads).
+template <int N> struct ZT {
+    static constexpr int L = 8;
+    static constexpr int E = Plan<N>::E;
+    static constexpr int T = N / E;
+    static constexpr int NT = L * T;
+    static constexpr int R0 = Plan<N>::R[0];
+    static constexpr int RL = Plan<N>::R[Plan<N>::NST - 1];
+    static constexpr int PP = N + 2;  // float2 per landed psi row (16-byte pad)
+    static constexpr int PF = N + 4;  // floats per landed phi row (16-byte pad)
+    static constexpr int NHP = half_pitch<float>(N);
+    static constexpr int PH = NHP + 2;  // float2 per landed half row (16-byte pad)
+    static constexpr size_t XCH = size_t(N) * L * sizeof(float2);  // [n][l] exchange tile
+    // P1 slot: 8 psi rows, then 8 phi rows
+    static constexpr size_t PSI_B = size_t(L) * PP * sizeof(float2);
+    static constexpr size_t SLOT1 = (PSI_B + size_t(L) * PF * sizeof(float) + 127) / 128 * 128;
+    // P5 slot: 8 psi rows
+    static constexpr size_t SLOT5 = (PSI_B + 127) / 128 * 128;
+    // P9 slot: 16 half rows
+    static constexpr size_t SLOT9 = (size_t(2 * L) * PH * sizeof(float2) + 127) / 128 * 128;
+    static_assert(XCH <= PSI_B && XCH <= SLOT9, "the exchange tile fits the landed rows");
+    static_assert(E == 8 && R0 == 8 && RL == 8, "register chain with radix-8 ends");
+    static_assert((N * sizeof(float2)) % 16 == 0 && (NHP * sizeof(float2)) % 16 == 0 &&
+                      (PP * sizeof(float2)) % 16 == 0 && (PF * sizeof(float)) % 16 == 0 &&
+                      (PH * sizeof(float2)) % 16 == 0,
+                  "bulk copies need 16-byte sizes and destinations");
+};
+
+template <int ST> __device__ __forceinline__ void ring_init(uint64_t *bar) {
+    if (threadIdx.x == 0) {
+        for (int s = 0; s < ST; ++s) mbar_init(&bar[s], 1);
+        mbar_init_fence();
+    }
+    __syncthreads();
+}
+
+// Bounded wait for tile i of the ring; on failure waits (bounded) for the
+// copies still in flight and returns false for the whole CTA.
+template <int ST> __device__ __forceinline__ bool ring_wait(uint64_t *bar, int i, int my_n, int *err) {
+    const bool ok = mbar_wait(&bar[i % ST], (uint32_t)((i / ST) & 1), err, 2);
+    if (__syncthreads_and(ok)) return true;
+    if (threadIdx.x == 0)
+        for (int j = i; j < my_n && j <= i + ST - 1; ++j) mbar_wait(&bar[j % ST], (uint32_t)((j / ST) & 1), err, 2);
+    __syncthreads();
+    return false;
+}
+
+__device__ __forceinline__ int ztiles_of_block(int ntiles) {
+    return (int)blockIdx.x < ntiles ? (ntiles - 1 - (int)blockIdx.x) / (int)gridDim.x + 1 : 0;
+}
+
+// ------------------------------------------------------------------- P1 ---
+template <int N, int ST, int MINB>
+__global__ void __launch_bounds__(ZT<N>::NT, MINB)
+    k_kick_fft_z_tma(float2 *__restrict__ psi, const float *__restrict__ phi, TState *__restrict__ ts,
+                     const float2 *__restrict__ tw, int ntiles) {
+    using Z = ZT<N>;
+    using C = float2;
+    constexpr int L = Z::L, T = Z::T, E = Z::E, R0 = Z::R0, RL = Z::RL;
+    extern __shared__ __align__(128) unsigned char smraw[];
+    uint64_t *bar = reinterpret_cast<uint64_t *>(smraw + ST * Z::SLOT1);
+    const int tid = threadIdx.x, l = tid % L, t = tid / L;
+    ring_init<ST>(bar);
+    const int my_n = ztiles_of_block(ntiles);
+    auto issue = [&](int i) {
+        const size_t row0 = size_t(blockIdx.x + (long)i * gridDim.x) * L;
+        unsigned char *slot = smraw + size_t(i % ST) * Z::SLOT1;
+        uint64_t *b = &bar[i % ST];
+        mbar_arrive_expect_tx(b, (uint32_t)(L * N * (sizeof(float2) + sizeof(float))));
+#pragma unroll 1
+        for (int r = 0; r < L; ++r) {
+            bulk_load(slot + size_t(r) * Z::PP * sizeof(float2), psi + (row0 + r) * N, N * sizeof(float2), b);
+            bulk_load(slot + Z::PSI_B + size_t(r) * Z::PF * sizeof(float), phi + (row0 + r) * N, N * sizeof(float),
+                      b);
+        }
+    };
+    if (tid == 0)
+        for (int i = 0; i < ST - 1 && i < my_n; ++i) issue(i);
+    const double cp = ts->coefP, cq = ts->coefQ, alpha = ts->alpha;
+    const C c0 = mkc((float)ts->cre, (float)ts->cim);
+    for (int i = 0; i < my_n; ++i) {
+        if (tid == 0 && i + ST - 1 < my_n) issue(i + ST - 1);
+        if (!ring_wait<ST>(bar, i, my_n, &ts->err)) return;
+        unsigned char *slot = smraw + size_t(i % ST) * Z::SLOT1;
+        const C *lp = reinterpret_cast<const C *>(slot) + l * Z::PP;
+        const float *lf = reinterpret_cast<const float *>(slot + Z::PSI_B) + l * Z::PF;
+        C v[E];
+#pragma unroll
+        for (int r = 0; r < R0; ++r) {
+            const int n = t + r * (N / R0);
+            const C g = lp[n];
+            const double p = cp * (double)lf[n] + cq * (double)cnorm2(g) + alpha;
+            v[r] = cmul(g, expmi<float>(p)) - c0;
+        }
+        stage_compute<C, N, E, -1, R0, 1>(v, tw, t);
+        RegChain<C, N, E, -1, L, L, 1, R0, 1>::run(reinterpret_cast<C *>(slot), v, tw, l, t, true);
+        C *out = psi + (size_t(blockIdx.x + (long)i * gridDim.x) * L + l) * N;
+#pragma unroll
+        for (int r = 0; r < RL; ++r) out[t + r * (N / RL)] = v[r];
+        fence_proxy_async_smem();
+        __syncthreads();
+    }
+}
+
+// ------------------------------------------------------------------- P5 ---
+template <int N, int ST, int MINB>
+__global__ void __launch_bounds__(ZT<N>::NT, MINB)
+    k_density_r2c_z_tma(float2 *__restrict__ psi, float2 *__restrict__ rhok, TState *__restrict__ ts,
+                        const float2 *__restrict__ tw, int ntiles) {
+    using Z = ZT<N>;
+    using C = float2;
+    constexpr int L = Z::L, T = Z::T, E = Z::E, R0 = Z::R0, RL = Z::RL, NT = Z::NT;
+    constexpr int M = N / 2, NHP = Z::NHP;
+    constexpr int LH = L / 2;  // packed complex lines of the density transform
+    extern __shared__ __align__(128) unsigned char smraw[];
+    uint64_t *bar = reinterpret_cast<uint64_t *>(smraw + ST * Z::SLOT5);
+    const int tid = threadIdx.x, l = tid % L, t = tid / L;
+    // the density transform: 4 lines, T threads each (whole warps: threads < LH * T)
+    const bool act = tid < LH * T;
+    const int p = tid % LH, tq = tid / LH;
+    ring_init<ST>(bar);
+    const int my_n = ztiles_of_block(ntiles);
+    auto issue = [&](int i) {
+        const size_t row0 = size_t(blockIdx.x + (long)i * gridDim.x) * L;
+        unsigned char *slot = smraw + size_t(i % ST) * Z::SLOT5;
+        uint64_t *b = &bar[i % ST];
+        mbar_arrive_expect_tx(b, (uint32_t)(L * N * sizeof(float2)));
+#pragma unroll 1
+        for (int r = 0; r < L; ++r)
+            bulk_load(slot + size_t(r) * Z::PP * sizeof(float2), psi + (row0 + r) * N, N * sizeof(float2), b);
+    };
+    if (tid == 0)
+        for (int i = 0; i < ST - 1 && i < my_n; ++i) issue(i);
+    const double mu = ts->mu;
+    const C c0 = mkc((float)ts->cre, (float)ts->cim);
+    double mx = 0.0;
+    for (int i = 0; i < my_n; ++i) {
+        if (tid == 0 && i + ST - 1 < my_n) issue(i + ST - 1);
+        if (!ring_wait<ST>(bar, i, my_n, &ts->err)) return;
+        unsigned char *slot = smraw + size_t(i % ST) * Z::SLOT5;
+        C *wk = reinterpret_cast<C *>(slot);
+        const size_t row0 = size_t(blockIdx.x + (long)i * gridDim.x) * L;
+        // inverse FFT of psi along z, stage 0 from the landed rows
+        C v[E];
+        const C *lp = reinterpret_cast<const C *>(slot) + l * Z::PP;
+#pragma unroll
+        for (int r = 0; r < R0; ++r) v[r] = lp[t + r * (N / R0)];
+        stage_compute<C, N, E, +1, R0, 1>(v, tw, t);
+        RegChain<C, N, E, +1, L, L, 1, R0, 1>::run(wk, v, tw, l, t, true);
+        // psi = IFFT + c; rho = |psi|^2 - mu into a float tile that pairs rows
+        // p and p+4 of element n: rt[(n*LH + p)*2 + h] holds row p + h*LH
+        // (conflict-free stores of the [l, t] layout and float2 loads of the
+        // packed layout)
+        float rho[RL];
+        C *out = psi + (row0 + l) * N;
+#pragma unroll
+        for (int r = 0; r < RL; ++r) {
+            const C g = v[r] + c0;
+            out[t + r * (N / RL)] = g;
+            const double n2 = (double)cnorm2(g);
+            mx = fmax(mx, n2);
+            rho[r] = (float)(n2 - mu);
+        }
+        float *rt = reinterpret_cast<float *>(slot);
+        __syncthreads();  // every thread is done with the exchange tile
+#pragma unroll
+        for (int r = 0; r < RL; ++r) rt[((t + r * (N / RL)) * LH + l % LH) * 2 + l / LH] = rho[r];
+        __syncthreads();
+        // packed lines rho_p + i rho_{p+4}, forward FFT (threads < LH*T)
+        if (act) {
+            const C *rp = reinterpret_cast<const C *>(rt);
+#pragma unroll
+            for (int r = 0; r < R0; ++r) v[r] = rp[(tq + r * (N / R0)) * LH + p];
+            stage_compute<C, N, E, -1, R0, 1>(v, tw, tq);
+        }
+        RegChain<C, N, E, -1, LH, LH, 1, R0, 3>::run(wk, v, tw, p, tq, act);
+        // Z_k in an [k][p] tile, then the two half spectra of each line
+        __syncthreads();
+        if (act) {
+#pragma unroll
+            for (int r = 0; r < RL; ++r) wk[(tq + r * (N / RL)) * LH + p] = v[r];
+        }
+        __syncthreads();
+        for (int q = tid; q < LH * (M + 1); q += NT) {
+            const int pp = q % LH, k = q / LH;
+            const C zk = wk[k * LH + pp];
+            const C zc = cconj(wk[((N - k) % N) * LH + pp]);
+            const C s = cscale(zk + zc, 0.5f);
+            const C d = cscale(zk - zc, 0.5f);
+            rhok[(row0 + pp) * NHP + k] = s;
+            rhok[(row0 + pp + LH) * NHP + k] = mkc(d.y, -d.x);
+        }
+        fence_proxy_async_smem();
+        __syncthreads();
+    }
+    mx = warp_max(mx);
+    if ((tid & 31) == 0 && my_n > 0) atomic_max_nonneg(&ts->maxrho_bits, mx);
+}
+
+// ------------------------------------------------------------------- P9 ---
+template <int N, int ST, int MINB>
+__global__ void __launch_bounds__(ZT<N>::NT, MINB)
+    k_c2r_z_tma(const float2 *__restrict__ rhok, float *__restrict__ phi, TState *__restrict__ ts, long win_rows,
+                int win_tail, const float2 *__restrict__ tw, int ntiles) {
+    using Z = ZT<N>;
+    using C = float2;
+    constexpr int L = Z::L, T = Z::T, E = Z::E, R0 = Z::R0, RL = Z::RL;
+    constexpr int M = N / 2, NHP = Z::NHP, ROWS = 2 * L;
+    extern __shared__ __align__(128) unsigned char smraw[];
+    uint64_t *bar = reinterpret_cast<uint64_t *>(smraw + ST * Z::SLOT9);
+    const int tid = threadIdx.x, l = tid % L, t = tid / L;
+    ring_init<ST>(bar);
+    const int my_n = ztiles_of_block(ntiles);
+    auto issue = [&](int i) {
+        const size_t row0 = size_t(blockIdx.x + (long)i * gridDim.x) * ROWS;
+        unsigned char *slot = smraw + size_t(i % ST) * Z::SLOT9;
+        uint64_t *b = &bar[i % ST];
+        mbar_arrive_expect_tx(b, (uint32_t)(ROWS * NHP * sizeof(float2)));
+#pragma unroll 1
+        for (int r = 0; r < ROWS; ++r)
+            bulk_load(slot + size_t(r) * Z::PH * sizeof(float2), rhok + (row0 + r) * NHP, NHP * sizeof(float2), b);
+    };
+    if (tid == 0)
+        for (int i = 0; i < ST - 1 && i < my_n; ++i) issue(i);
+    constexpr KSplit<float> inv(1.0 / ((double)N * N * N));
+    double mx = 0.0;  // the running max on the FP64 pipe, which this pass leaves idle
+    for (int i = 0; i < my_n; ++i) {
+        if (tid == 0 && i + ST - 1 < my_n) issue(i + ST - 1);
+        if (!ring_wait<ST>(bar, i, my_n, &ts->err)) return;
+        unsigned char *slot = smraw + size_t(i % ST) * Z::SLOT9;
+        const C *xa = reinterpret_cast<const C *>(slot) + l * Z::PH;
+        const C *xb = xa + L * Z::PH;
+        C v[E];
+#pragma unroll
+        for (int r = 0; r < R0; ++r) {
+            const int n = t + r * (N / R0);
+            const int m = n <= M ? n : N - n;
+            C a = xa[m], b = xb[m];
+            if (m == 0 || m == M) {  // c2r ignores these imaginary parts
+                a.y = 0.f;
+                b.y = 0.f;
+            }
+            v[r] = n <= M ? mkc(a.x - b.y, a.y + b.x) : mkc(a.x + b.y, b.x - a.y);
+        }
+        stage_compute<C, N, E, +1, R0, 1>(v, tw, t);
+        RegChain<C, N, E, +1, L, L, 1, R0, 1>::run(reinterpret_cast<C *>(slot), v, tw, l, t, true);
+        const long ra = long(blockIdx.x + (long)i * gridDim.x) * ROWS + l, rb = ra + L;
+        // elements of rows below win_rows, and the first win_tail of row win_rows, are in the window
+        const int lima = ra < win_rows ? N : (ra == win_rows ? win_tail : 0);
+        const int limb = rb < win_rows ? N : (rb == win_rows ? win_tail : 0);
+        float *oa = phi + size_t(ra) * N, *ob = phi + size_t(rb) * N;
+#pragma unroll
+        for (int r = 0; r < RL; ++r) {
+            const int n = t + r * (N / RL);
+            const float fa = mulk(v[r].x, inv.hi, inv.lo), fb = mulk(v[r].y, inv.hi, inv.lo);
+            oa[n] = fa;
+            ob[n] = fb;
+            if (n < lima) mx = fmax(mx, (double)fabsf(fa));
+            if (n < limb) mx = fmax(mx, (double)fabsf(fb));
+        }
+        fence_proxy_async_smem();
+        __syncthreads();
+    }
+    const double m = warp_max(mx);
+    if ((tid & 31) == 0) atomic_max_nonneg(&ts->maxphi_bits, m);
+}
+
+}  // namespace ifdm

@@ -253,8 +253,11 @@ int ifdm_fft3d(void *data, int n, int precision, int sign, void *stream);
  * IFDM_STATIC_MAX_RES (16, 32, 48, 64); larger sizes return
  * IFDM_ERR_UNSUPPORTED.  All calls share that array: calls that overlap on
  * the GPU (other streams, other host threads) race and must be serialised by
- * the caller.  The first call on a device looks up the array's address
- * (cudaGetSymbolAddress); make it before any stream capture. */
+ * the caller.  The first call on a device, whatever its res, does that
+ * device's one-time set-up: it looks up the array's address
+ * (cudaGetSymbolAddress) and sets the kernels' shared-memory attributes for
+ * every supported res; make it before any stream capture.  res <= 0 or a null
+ * pointer returns IFDM_ERR_ARGS. */
 #define IFDM_STATIC_SCRATCH_BYTES (3u << 20)
 #define IFDM_STATIC_MAX_RES 64
 int ifdm_poisson_static(const double *psi, double *phi, int res, double mfdm, double xmax, void *stream);

@@ -60,7 +60,9 @@ def run_case(name, stan, N, seed, g, t_write, t_stop, keep):
             if f not in keep and f != "voutput.dat":
                 os.remove(os.path.join(out, f))
         files = sorted(f for f in os.listdir(out) if f.endswith(".dat"))
-    return {"binary": os.path.basename(ref_binary(stan)), "args": ["<ic>" if a == icdir else a for a in args],
+    # paths are recorded relative to this folder: the output prefix as <golden>/<case>/
+    rec = ["<ic>" if a == icdir else a.replace(HERE + "/", "<golden>/") for a in args]
+    return {"binary": os.path.basename(ref_binary(stan)), "args": rec,
             "ic": os.path.basename(icdir), "files": files}
 
 

@@ -34,45 +34,62 @@ def _loss(psi, target_logrho):
     return ((torch.log(psi.abs() ** 2 / S**2) - target_logrho) ** 2).mean()
 
 
-def _target(n, nsteps, dt_scale, prec):
+def _g_for(n, dt_scale, phase):
+    """g whose kick turns the densest cell of the seed-11 IC by `phase` radians in the first step."""
+    import bench
+
+    return bench.g_for_phase(n, zeldovich_psi(n, seed=11), dt_scale, phase)
+
+
+def _target(n, nsteps, dt_scale, prec, g=0.0):
     import torch
 
     tgt = torch.from_numpy(zeldovich_psi(n, seed=12)).cuda()
-    sim = ifdm.Simulation(MFDM, 0.0, XMAX, n, precision=prec)
+    sim = ifdm.Simulation(MFDM, g, XMAX, n, precision=prec)
     with torch.no_grad():
         t_out = evolve(tgt, sim, A0, nsteps, dt_scale, 7)
     sim.close()
     return torch.log(t_out.abs() ** 2 / S**2)
 
 
-def _assert_kinetic_schedule(n, nsteps, dt_scale):
+def _first_non_kinetic_step(n, nsteps, dt_scale, g=0.0):
+    """Index of the first step not limited by the kinetic criterion, or None."""
     psi0 = zeldovich_psi(n, seed=11)
-    with ifdm.Simulation(MFDM, 0.0, XMAX, n) as sim:
+    with ifdm.Simulation(MFDM, g, XMAX, n) as sim:
         sim.set_psi(psi0, A0)
-        for _ in range(nsteps):
+        for i in range(nsteps):
             sim.step(1, dt_scale)
-            assert sim.state()["criterion"] == 3, "a step was not limited by the kinetic criterion"
+            if sim.state()["criterion"] != 3:
+                return i
+    return None
 
 
-def _gradient(n, nsteps, dt_scale, ckpt, prec, target):
+def _assert_kinetic_schedule(n, nsteps, dt_scale, g=0.0):
+    assert _first_non_kinetic_step(n, nsteps, dt_scale, g) is None, "a step was not limited by the kinetic criterion"
+
+
+def _gradient(n, nsteps, dt_scale, ckpt, prec, target, g=0.0):
     import torch
 
     psi0 = torch.from_numpy(zeldovich_psi(n, seed=11)).cuda()
-    sim = ifdm.Simulation(MFDM, 0.0, XMAX, n, precision=prec)
+    sim = ifdm.Simulation(MFDM, g, XMAX, n, precision=prec)
     x = psi0.clone().requires_grad_(True)
     _loss(evolve(x, sim, A0, nsteps, dt_scale, ckpt), target).backward()
     sim.close()
     return psi0, x.grad.detach() * S  # gradient in the scaled field psi/S
 
 
-def _fd_check(n, nsteps, dt_scale, ckpt, prec, tol, ndir):
+def _fd_check(n, nsteps, dt_scale, ckpt, prec, tol, ndir, gsi=0.0):
+    """Adjoint of `prec` against FP64 central differences along ndir directions;
+    returns the worst relative disagreement."""
     import torch
 
-    target = _target(n, nsteps, dt_scale, "fp64")
-    psi0, g = _gradient(n, nsteps, dt_scale, ckpt, prec, target)
-    sim = ifdm.Simulation(MFDM, 0.0, XMAX, n, precision="fp64")
+    target = _target(n, nsteps, dt_scale, "fp64", gsi)
+    psi0, g = _gradient(n, nsteps, dt_scale, ckpt, prec, target, gsi)
+    sim = ifdm.Simulation(MFDM, gsi, XMAX, n, precision="fp64")
     rng = np.random.default_rng(3)
     eps = 1e-3
+    worst = 0.0
     for _ in range(ndir):
         d = rng.standard_normal((n, n, n)) + 1j * rng.standard_normal((n, n, n))
         d = torch.from_numpy(d / np.linalg.norm(d)).cuda()
@@ -82,8 +99,10 @@ def _fd_check(n, nsteps, dt_scale, ckpt, prec, tol, ndir):
         fd = (lp - lm) / (2 * eps)
         adj = float(torch.sum(g.real * d.real + g.imag * d.imag).item())
         err = abs(fd - adj) / max(abs(fd), abs(adj))
+        worst = max(worst, err)
         assert err <= tol, (fd, adj, err)
     sim.close()
+    return worst
 
 
 @pytest.mark.parametrize("prec,tol", [("fp64", 2e-5), ("mixed", 2e-3)])
@@ -104,6 +123,59 @@ def test_adjoint_128_200_steps_mixed():
     n, nsteps, C, ckpt = 128, 200, 0.05, 20
     _assert_kinetic_schedule(n, nsteps, C)
     _fd_check(n, nsteps, C, ckpt, "mixed", 5e-3, ndir=16)
+
+
+@pytest.mark.parametrize("prec,tol", [("fp64", 2e-5), ("mixed", 2e-3), ("fp32", 5e-3)])
+def test_adjoint_with_self_interaction_matches_finite_differences(prec, tol):
+    """The linearised g|psi|^2 term of the kick: g set so that the densest
+    cell turns by 0.1 rad in the first step (the self-interaction strength of
+    the 512^3 precision configuration), every step still kinetic-limited."""
+    n, nsteps, C, ckpt = 64, 24, 0.05, 7
+    g = _g_for(n, C, 0.1)
+    _assert_kinetic_schedule(n, nsteps, C, g)
+    worst = _fd_check(n, nsteps, C, ckpt, prec, tol, ndir=16, gsi=g)
+    print(f"g={g:.4e} {prec}: worst adjoint/FD disagreement {worst:.2e}")
+
+
+def test_self_interaction_term_changes_the_gradient():
+    """The g|psi|^2 term is not negligible in the test above: the gradient with
+    g differs from the one without by far more than the FD tolerance."""
+    n, nsteps, C = 64, 24, 0.05
+    g = _g_for(n, C, 0.1)
+    t0 = _target(n, nsteps, C, "fp64", 0.0)
+    _, g0 = _gradient(n, nsteps, C, 7, "fp64", t0, 0.0)
+    _, g1 = _gradient(n, nsteps, C, 7, "fp64", t0, g)
+    d = float((g1 - g0).abs().norm() / g0.abs().norm())
+    print(f"gradient change from the self-interaction term: {d:.3e}")
+    assert d > 1e-2
+
+
+def test_adjoint_differentiation_config_fp32():
+    """The differentiation configuration on the FP32 path: 128^3, 200 steps,
+    checkpoints every 20 steps, 16 directions, eps = 1e-3, against FP64
+    central differences and against the FP64 adjoint.
+
+    The configuration's own schedule (the step scale that reaches a = 0.5 in
+    200 steps, 0.22) hands some steps to the potential criterion, whose step
+    size depends on max|phi| and is not differentiated; the test uses the
+    largest scale of a fixed ladder at which all 200 steps stay kinetic-limited
+    and prints where the larger ones leave it."""
+    n, nsteps, ckpt = 128, 200, 20
+    C = None
+    for c in (0.22, 0.15, 0.1, 0.07, 0.05):
+        first = _first_non_kinetic_step(n, nsteps, c)
+        print(f"128^3 step scale {c}: first non-kinetic step {first}")
+        if first is None:
+            C = c
+            break
+    assert C is not None
+    worst = _fd_check(n, nsteps, C, ckpt, "fp32", 2e-2, ndir=16)
+    target = _target(n, nsteps, C, "fp64")
+    _, g64 = _gradient(n, nsteps, C, ckpt, "fp64", target)
+    _, g32 = _gradient(n, nsteps, C, ckpt, "fp32", target)
+    e = float((g32 - g64).abs().norm() / g64.abs().norm())
+    print(f"128^3/200 steps, C={C}: fp32 adjoint vs FD worst {worst:.2e}, vs FP64 adjoint {e:.2e}")
+    assert e <= 2e-2
 
 
 def test_reduced_precision_adjoint_close_to_fp64():

@@ -1,0 +1,114 @@
+"""The benchmarked 512^3 configuration against the oracle (needs a B200).
+
+Several kernel variants run only at N = 512: the 8 x 8 x 8 radix plan, the
+8-line FP32 y/x tiles with the 64-register cap and the slot swizzle, the
+4-line FP64 y tiles, the cp.async-pipelined FP32 density pass and the radix-4
+256-point half transform of the FP32 real-to-complex pass.  These tests hold
+each of them to the oracle (the C restatement of src/CosmoBEC_MPI.cpp) or to
+numpy on the benchmark's own inputs:
+
+* the stand-alone 3-D FFT at n = 512 against numpy, complex128 and complex64;
+* two fixed-mode leap-frog steps of the benchmark configuration (512^3,
+  xmax 5, mfdm 2.5e-24 eV, self-interaction at 0.01 rad per step at the
+  densest cell, the step scale that reaches a = 0.5 in 1000 steps) in every
+  precision mode, through the TMA passes and through the plain passes, against
+  the oracle's two steps from the same psi;
+* phi of the initial Poisson solve against the oracle's.
+
+The oracle needs about 7 GB of host memory and ~7 s per step on 16 cores at
+this size; it runs once per module.
+"""
+
+import numpy as np
+import pytest
+
+import ifdm_code_b200 as ifdm
+from ifdm_code_b200 import Simulation
+from oracle import Oracle, OracleArgs
+from tests.snapshot_util import rel_l2
+
+pytestmark = pytest.mark.gpu
+
+N = 512
+STEPS = 2
+PSI_TOL = 1e-10  # FP64 drop-in bar
+# reduced precision after two steps: psi relative L2 (phase errors included)
+REDUCED_TOL = {"fp32": 2e-5, "mixed": 2e-6}
+
+
+@pytest.fixture(scope="module")
+def case512():
+    import bench
+    from ifdm_code_b200.synthetic_ic import zeldovich_psi
+
+    psi0 = zeldovich_psi(N, xmax=bench.XMAX, seed=0, a=bench.A0, mfdm=bench.MFDM)
+    C = bench.dt_scale_for(N)
+    g = bench.g_for_phase(N, psi0, C, 0.01)
+    o = Oracle(OracleArgs(res=N, mfdm=bench.MFDM, g=g, xmax=bench.XMAX))
+    o.set_psi(psi0, bench.A0)
+    o.poisson()
+    phi0 = o.phi()
+    o.run_fixed(STEPS, C)
+    ref = o.psi()
+    a_ref = o.a
+    o.close()
+    return dict(psi0=psi0, C=C, g=g, phi0=phi0, ref=ref, a=a_ref, A0=bench.A0, xmax=bench.XMAX, mfdm=bench.MFDM)
+
+
+def _run(case, prec, tma, monkeypatch):
+    if tma:
+        monkeypatch.delenv("IFDM_NO_TMA", raising=False)
+    else:
+        monkeypatch.setenv("IFDM_NO_TMA", "1")
+    with Simulation(case["mfdm"], case["g"], case["xmax"], N, precision=prec) as s:
+        s.set_psi(case["psi0"], case["A0"])
+        phi = s.get_phi() if prec == "fp64" else None
+        s.step(STEPS, case["C"])
+        psi = s.get_psi()
+        st = s.state()
+    return psi, phi, st
+
+
+@pytest.mark.parametrize("tma", [True, False], ids=["tma", "plain"])
+def test_fp64_512_matches_oracle(case512, tma, monkeypatch):
+    psi, phi, st = _run(case512, "fp64", tma, monkeypatch)
+    assert st["device_error"] == 0
+    assert st["steps"] == STEPS and st["a"] == pytest.approx(case512["a"], rel=1e-12)
+    assert rel_l2(phi, case512["phi0"]) <= 1e-12
+    err = rel_l2(psi, case512["ref"])
+    print(f"fp64 512^3 {'tma' if tma else 'plain'}: psi rel L2 vs oracle {err:.3e}")
+    assert err <= PSI_TOL
+
+
+@pytest.mark.parametrize("tma", [True, False], ids=["tma", "plain"])
+@pytest.mark.parametrize("prec", ["fp32", "mixed"])
+def test_reduced_precision_512_matches_oracle(case512, prec, tma, monkeypatch):
+    psi, _, st = _run(case512, prec, tma, monkeypatch)
+    assert st["device_error"] == 0
+    assert st["a"] == pytest.approx(case512["a"], rel=1e-6)
+    err = rel_l2(psi, case512["ref"])
+    print(f"{prec} 512^3 {'tma' if tma else 'plain'}: psi rel L2 vs oracle {err:.3e}")
+    assert err <= REDUCED_TOL[prec]
+
+
+def test_fft3d_512_matches_numpy():
+    import scipy.fft as sfft
+    import torch
+
+    rng = np.random.default_rng(512)
+    x = rng.standard_normal((N, N, N)) + 1j * rng.standard_normal((N, N, N))
+    ref = sfft.fftn(x, workers=-1)
+    for dt, tol, comp in ((torch.complex128, 1e-13, None), (torch.complex64, 2e-6, None),
+                          (torch.complex64, 2e-7, "fp64")):
+        t = torch.from_numpy(x).to(dt).cuda()
+        ifdm.fft3d_(t, -1, comp)
+        torch.cuda.synchronize()
+        err = rel_l2(t.cpu().numpy(), ref)
+        assert err <= tol, (dt, comp, err)
+        ifdm.fft3d_(t, +1, comp)
+        torch.cuda.synchronize()
+        back = t.cpu().numpy() / N**3
+        err = rel_l2(back, x)
+        assert err <= tol, (dt, comp, err)
+        del t
+        torch.cuda.empty_cache()

@@ -61,6 +61,9 @@ template <> struct Plan<96> { static constexpr int E = 12, NST = 4; static const
 template <> struct Plan<128> { static constexpr int E = 8, NST = 3; static constexpr int R[3] = {8, 2, 8}; };
 template <> struct Plan<256> { static constexpr int E = 8, NST = 3; static constexpr int R[3] = {8, 4, 8}; };
 template <> struct Plan<512> { static constexpr int E = 8, NST = 3; static constexpr int R[3] = {8, 8, 8}; };
+// 1024 = 4 * 8 * 8 * 4: radix-4 ends keep the first and last radix equal
+// (chained transforms) with 8 elements per thread
+template <> struct Plan<1024> { static constexpr int E = 8, NST = 4; static constexpr int R[4] = {4, 8, 8, 4}; };
 
 // Alternative radix orders with the same elements per thread (V = 1), for the
 // batch autotuner; V = 0 and sizes without an alternative are Plan<N>.

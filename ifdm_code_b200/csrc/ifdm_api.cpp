@@ -86,10 +86,7 @@ int ifdm_params_from_argv(int argc, char **argv, ifdm_params *p) {
     return IFDM_OK;
 }
 
-int ifdm_supported_res(int res, int precision) {
-    (void)precision;
-    return supported_n(res) ? 1 : 0;
-}
+int ifdm_supported_res(int res, int precision) { return supported_n(res, precision) ? 1 : 0; }
 
 int ifdm_create(const ifdm_params *p, ifdm_ctx **out) {
     if (!p || !out) return IFDM_ERR_ARGS;
@@ -100,13 +97,14 @@ int ifdm_create(const ifdm_params *p, ifdm_ctx **out) {
     c->icpath = p->icpath ? p->icpath : "";
     c->p.opath = c->opath.c_str();
     c->p.icpath = c->icpath.c_str();
-    if (!supported_n(p->res)) {
-        *out = c.release();
-        return fail(*out, IFDM_ERR_UNSUPPORTED, "res " + std::to_string(p->res) + " has no compiled FFT plan");
-    }
     if (p->precision != IFDM_FP64 && p->precision != IFDM_FP32 && p->precision != IFDM_MIXED) {
         *out = c.release();
         return fail(*out, IFDM_ERR_ARGS, "precision must be IFDM_FP64, IFDM_FP32 or IFDM_MIXED");
+    }
+    if (!supported_n(p->res, p->precision)) {
+        *out = c.release();
+        return fail(*out, IFDM_ERR_UNSUPPORTED,
+                    "res " + std::to_string(p->res) + " has no compiled FFT plan in this precision mode");
     }
     using namespace phys;
     c->N = p->res;
@@ -681,7 +679,7 @@ void ifdm_batch_destroy(ifdm_batch *b) {
 
 int ifdm_fft3d(void *data, int n, int precision, int sign, void *stream) {
     if (!data || (sign != 1 && sign != -1) || precision < 0 || precision > 2) return IFDM_ERR_ARGS;
-    if (!supported_n(n)) return IFDM_ERR_UNSUPPORTED;
+    if (!supported_n(n, precision)) return IFDM_ERR_UNSUPPORTED;
     std::string e = fft3d(data, n, precision, sign, (cudaStream_t)stream);
     return e.empty() ? IFDM_OK : IFDM_ERR_CUDA;
 }

@@ -41,9 +41,14 @@ const char *const kPassNames[kNumPasses] = {
 
 bool supported_n(int n) {
     switch (n) {
-        case 16: case 32: case 48: case 64: case 96: case 128: case 256: case 512: return true;
+        case 16: case 32: case 48: case 64: case 96: case 128: case 256: case 512: case 1024: return true;
         default: return false;
     }
+}
+
+bool supported_n(int n, int precision) {
+    if (precision == 2 && n >= 1024) return false;  // mixed: FP64 exchange tiles exceed shared memory
+    return supported_n(n);
 }
 
 // ---------------------------------------------------------------- per-N ops --
@@ -134,11 +139,11 @@ template <typename R_, typename K_, int N> struct Box {
     // but slowed the FP64 z passes (one 2-slot block per SM hides less latency
     // than three plain blocks), and pipelined P1/P9 gained nothing.
     static constexpr bool kTma = N >= 128;
-    static constexpr bool kZPipe = N >= 128 && std::is_same<R, float>::value && std::is_same<K, float>::value;
+    static constexpr bool kZPipe = N >= 128 && N <= 512 && std::is_same<R, float>::value && std::is_same<K, float>::value;
     // FP32 z passes fed by bulk copies (zpass_tma.cuh) for N >= 256; ring
     // depth and resident blocks per SM of P1, P5 and P9
     static constexpr bool kZT = N >= 256 && std::is_same<R, float>::value && std::is_same<K, float>::value;
-    static constexpr int ZST1 = 2, ZB1 = 2, ZST5 = 3, ZB5 = 2, ZST9 = 3, ZB9 = 2;
+    static constexpr int ZST1 = 2, ZST5 = 3, ZST9 = 3, ZB1 = N >= 1024 ? 1 : 2, ZB5 = ZB1, ZB9 = ZB1;
     static constexpr size_t ZSM1 = kZT ? ZST1 * ZT<(kZT ? N : 256)>::SLOT1 + 64 : 0;
     static constexpr size_t ZSM5 = kZT ? ZST5 * ZT<(kZT ? N : 256)>::SLOT5 + 64 : 0;
     static constexpr size_t ZSM9 = kZT ? ZST9 * ZT<(kZT ? N : 256)>::SLOT9 + 64 : 0;
@@ -264,6 +269,10 @@ template <typename R, typename K, typename F> static std::string with_box(int n,
         case 128: return f(Box<R, K, 128>{});
         case 256: return f(Box<R, K, 256>{});
         case 512: return f(Box<R, K, 512>{});
+        case 1024:
+            // the mixed mode's FP64 exchange tiles do not fit shared memory at 1024
+            if constexpr (std::is_same<R, K>::value) return f(Box<R, K, 1024>{});
+            else return "grid size 1024 is not supported in mixed precision";
         default: return "unsupported grid size " + std::to_string(n);
     }
 }
@@ -407,7 +416,7 @@ std::string StepEngine::init(const EngineConfig &cfg, cudaStream_t stream) {
     cfg_ = cfg;
     stream_ = stream;
     const int N = cfg.N;
-    if (!supported_n(N)) return "unsupported grid size " + std::to_string(N);
+    if (!supported_n(N, cfg.precision)) return "unsupported grid size " + std::to_string(N);
     const size_t n3 = n3_();
     const size_t rs = storage_bytes(cfg.precision), cs = 2 * rs;
     const int nhp = cfg.precision == 0 ? half_pitch<double>(N) : half_pitch<float>(N);
@@ -864,7 +873,7 @@ std::string StepEngine::adjoint(const double *g_final_dev, double *g0_dev) {
 }
 
 std::string fft3d(void *data, int n, int precision, int sign, cudaStream_t stream) {
-    if (!supported_n(n)) return "unsupported grid size " + std::to_string(n);
+    if (!supported_n(n, precision)) return "unsupported grid size " + std::to_string(n);
     void *tw = nullptr;
     std::string e = get_twiddles(n, compute_kind(precision), &tw);
     if (!e.empty()) return e;

@@ -47,7 +47,11 @@ template <typename R, typename K, int N, bool ZR = false> struct Tile {
     static constexpr int GB = (int)sizeof(G);
     static constexpr int PH = sizeof(C) == 16 ? 8 : 16;            // threads per smem phase
     static constexpr int LC = ZR ? 1 : 128 / GB;                    // lines for 128-byte rows
-    static constexpr int E0 = Plan<N>::E * ((!ZR && sizeof(C) == 16 && GB == 8 && N >= 256) ? 2 : 1);
+    // elements per thread: the plan's, doubled for mixed y/x lines at N >= 256
+    // and for every tile at N >= 1024 (the lines of a 1024-point tile would
+    // otherwise need more than 1024 threads)
+    static constexpr int E0 = Plan<N>::E * ((!ZR && sizeof(C) == 16 && GB == 8 && N >= 256) ? 2 : 1) *
+                              (N >= 1024 ? 2 : 1);
     static constexpr int T = N / E0;                                // threads per line
     static constexpr int LT = 256 / T;                              // lines for >= 256 threads
     static constexpr int L1 = LT > LC ? LT : LC;

@@ -42,8 +42,14 @@ template <typename R, typename K, int N, int AXIS = 1> struct TmaTile {
     // 0.89 -> 0.85 ms, P6/P8 0.50 -> 0.45 ms; the FP64 x passes measured
     // slower that way: P3 1.39 -> 1.93 ms, P7 0.71 -> 0.78 ms)
     static constexpr bool NARROW64 = !SPLIT && sizeof(G) == 16 && AXIS == 1 && N >= 512;
-    static constexpr int MINB = ((NARROW && AXIS == 1) || NARROW64) ? 2 : 1;  // resident blocks the registers must allow
-    static constexpr int L = NARROW64 ? 4 : (SPLIT || NARROW) ? 8 : 128 / (int)sizeof(G);
+    // N = 1024 (128 threads per line): one block per SM holds the ring; the
+    // x tiles (two chained transforms) take half the y tiles' lines, FP32 4
+    // and FP64 2, which keeps them within the registers of their block size
+    // (8 FP32 lines spilled 344 bytes a thread at 64 registers)
+    static constexpr bool BIG = N >= 1024;
+    static constexpr int MINB = BIG ? 1 : ((NARROW && AXIS == 1) || NARROW64) ? 2 : 1;  // resident blocks the registers must allow
+    static constexpr int L = BIG ? (sizeof(G) == 16 ? 4 : 8) / (AXIS == 2 ? 2 : 1)
+                                 : NARROW64 ? 4 : (SPLIT || NARROW) ? 8 : 128 / (int)sizeof(G);
     static constexpr bool SWZ = NARROW || NARROW64;  // slot swizzle of the exchange tile
     static constexpr int E = Plan<N>::E;
     static constexpr int T = N / E;

@@ -57,7 +57,7 @@ template <int N> struct ZT {
     // P9 slot: 16 half rows
     static constexpr size_t SLOT9 = (size_t(2 * L) * PH * sizeof(float2) + 127) / 128 * 128;
     static_assert(XCH <= PSI_B && XCH <= SLOT9, "the exchange tile fits the landed rows");
-    static_assert(E == 8 && R0 == 8 && RL == 8, "register chain with radix-8 ends");
+    static_assert(E % R0 == 0 && E % RL == 0 && R0 == RL, "register chain: equal first and last radix");
     static_assert((N * sizeof(float2)) % 16 == 0 && (NHP * sizeof(float2)) % 16 == 0 &&
                       (PP * sizeof(float2)) % 16 == 0 && (PF * sizeof(float)) % 16 == 0 &&
                       (PH * sizeof(float2)) % 16 == 0,
@@ -124,17 +124,21 @@ __global__ void __launch_bounds__(ZT<N>::NT, MINB)
         const float *lf = reinterpret_cast<const float *>(slot + Z::PSI_B) + l * Z::PF;
         C v[E];
 #pragma unroll
-        for (int r = 0; r < R0; ++r) {
-            const int n = t + r * (N / R0);
-            const C g = lp[n];
-            const double p = cp * (double)lf[n] + cq * (double)cnorm2(g) + alpha;
-            v[r] = cmul(g, expmi<float>(p)) - c0;
-        }
+        for (int b = 0; b < E / R0; ++b)
+#pragma unroll
+            for (int r = 0; r < R0; ++r) {
+                const int n = t + T * b + r * (N / R0);
+                const C g = lp[n];
+                const double p = cp * (double)lf[n] + cq * (double)cnorm2(g) + alpha;
+                v[b * R0 + r] = cmul(g, expmi<float>(p)) - c0;
+            }
         stage_compute<C, N, E, -1, R0, 1>(v, tw, t);
         RegChain<C, N, E, -1, L, L, 1, R0, 1>::run(reinterpret_cast<C *>(slot), v, tw, l, t, true);
         C *out = psi + (size_t(blockIdx.x + (long)i * gridDim.x) * L + l) * N;
 #pragma unroll
-        for (int r = 0; r < RL; ++r) out[t + r * (N / RL)] = v[r];
+        for (int b = 0; b < E / RL; ++b)
+#pragma unroll
+            for (int r = 0; r < RL; ++r) out[t + T * b + r * (N / RL)] = v[b * RL + r];
         fence_proxy_async_smem();
         __syncthreads();
     }
@@ -182,33 +186,42 @@ __global__ void __launch_bounds__(ZT<N>::NT, MINB)
         C v[E];
         const C *lp = reinterpret_cast<const C *>(slot) + l * Z::PP;
 #pragma unroll
-        for (int r = 0; r < R0; ++r) v[r] = lp[t + r * (N / R0)];
+        for (int b = 0; b < E / R0; ++b)
+#pragma unroll
+            for (int r = 0; r < R0; ++r) v[b * R0 + r] = lp[t + T * b + r * (N / R0)];
         stage_compute<C, N, E, +1, R0, 1>(v, tw, t);
         RegChain<C, N, E, +1, L, L, 1, R0, 1>::run(wk, v, tw, l, t, true);
         // psi = IFFT + c; rho = |psi|^2 - mu into a float tile that pairs rows
         // p and p+4 of element n: rt[(n*LH + p)*2 + h] holds row p + h*LH
         // (conflict-free stores of the [l, t] layout and float2 loads of the
         // packed layout)
-        float rho[RL];
+        float rho[E];
         C *out = psi + (row0 + l) * N;
 #pragma unroll
-        for (int r = 0; r < RL; ++r) {
-            const C g = v[r] + c0;
-            out[t + r * (N / RL)] = g;
-            const double n2 = (double)cnorm2(g);
-            mx = fmax(mx, n2);
-            rho[r] = (float)(n2 - mu);
-        }
+        for (int b = 0; b < E / RL; ++b)
+#pragma unroll
+            for (int r = 0; r < RL; ++r) {
+                const C g = v[b * RL + r] + c0;
+                out[t + T * b + r * (N / RL)] = g;
+                const double n2 = (double)cnorm2(g);
+                mx = fmax(mx, n2);
+                rho[b * RL + r] = (float)(n2 - mu);
+            }
         float *rt = reinterpret_cast<float *>(slot);
         __syncthreads();  // every thread is done with the exchange tile
 #pragma unroll
-        for (int r = 0; r < RL; ++r) rt[((t + r * (N / RL)) * LH + l % LH) * 2 + l / LH] = rho[r];
+        for (int b = 0; b < E / RL; ++b)
+#pragma unroll
+            for (int r = 0; r < RL; ++r)
+                rt[((t + T * b + r * (N / RL)) * LH + l % LH) * 2 + l / LH] = rho[b * RL + r];
         __syncthreads();
         // packed lines rho_p + i rho_{p+4}, forward FFT (threads < LH*T)
         if (act) {
             const C *rp = reinterpret_cast<const C *>(rt);
 #pragma unroll
-            for (int r = 0; r < R0; ++r) v[r] = rp[(tq + r * (N / R0)) * LH + p];
+            for (int b = 0; b < E / R0; ++b)
+#pragma unroll
+                for (int r = 0; r < R0; ++r) v[b * R0 + r] = rp[(tq + T * b + r * (N / R0)) * LH + p];
             stage_compute<C, N, E, -1, R0, 1>(v, tw, tq);
         }
         RegChain<C, N, E, -1, LH, LH, 1, R0, 3>::run(wk, v, tw, p, tq, act);
@@ -216,7 +229,9 @@ __global__ void __launch_bounds__(ZT<N>::NT, MINB)
         __syncthreads();
         if (act) {
 #pragma unroll
-            for (int r = 0; r < RL; ++r) wk[(tq + r * (N / RL)) * LH + p] = v[r];
+            for (int b = 0; b < E / RL; ++b)
+#pragma unroll
+                for (int r = 0; r < RL; ++r) wk[(tq + T * b + r * (N / RL)) * LH + p] = v[b * RL + r];
         }
         __syncthreads();
         for (int q = tid; q < LH * (M + 1); q += NT) {
@@ -270,16 +285,18 @@ __global__ void __launch_bounds__(ZT<N>::NT, MINB)
         const C *xb = xa + L * Z::PH;
         C v[E];
 #pragma unroll
-        for (int r = 0; r < R0; ++r) {
-            const int n = t + r * (N / R0);
-            const int m = n <= M ? n : N - n;
-            C a = xa[m], b = xb[m];
-            if (m == 0 || m == M) {  // c2r ignores these imaginary parts
-                a.y = 0.f;
-                b.y = 0.f;
+        for (int bb = 0; bb < E / R0; ++bb)
+#pragma unroll
+            for (int r = 0; r < R0; ++r) {
+                const int n = t + T * bb + r * (N / R0);
+                const int m = n <= M ? n : N - n;
+                C a = xa[m], b = xb[m];
+                if (m == 0 || m == M) {  // c2r ignores these imaginary parts
+                    a.y = 0.f;
+                    b.y = 0.f;
+                }
+                v[bb * R0 + r] = n <= M ? mkc(a.x - b.y, a.y + b.x) : mkc(a.x + b.y, b.x - a.y);
             }
-            v[r] = n <= M ? mkc(a.x - b.y, a.y + b.x) : mkc(a.x + b.y, b.x - a.y);
-        }
         stage_compute<C, N, E, +1, R0, 1>(v, tw, t);
         RegChain<C, N, E, +1, L, L, 1, R0, 1>::run(reinterpret_cast<C *>(slot), v, tw, l, t, true);
         const long ra = long(blockIdx.x + (long)i * gridDim.x) * ROWS + l, rb = ra + L;
@@ -288,14 +305,17 @@ __global__ void __launch_bounds__(ZT<N>::NT, MINB)
         const int limb = rb < win_rows ? N : (rb == win_rows ? win_tail : 0);
         float *oa = phi + size_t(ra) * N, *ob = phi + size_t(rb) * N;
 #pragma unroll
-        for (int r = 0; r < RL; ++r) {
-            const int n = t + r * (N / RL);
-            const float fa = mulk(v[r].x, inv.hi, inv.lo), fb = mulk(v[r].y, inv.hi, inv.lo);
-            oa[n] = fa;
-            ob[n] = fb;
-            if (n < lima) mx = fmax(mx, (double)fabsf(fa));
-            if (n < limb) mx = fmax(mx, (double)fabsf(fb));
-        }
+        for (int bb = 0; bb < E / RL; ++bb)
+#pragma unroll
+            for (int r = 0; r < RL; ++r) {
+                const int n = t + T * bb + r * (N / RL);
+                const C z = v[bb * RL + r];
+                const float fa = mulk(z.x, inv.hi, inv.lo), fb = mulk(z.y, inv.hi, inv.lo);
+                oa[n] = fa;
+                ob[n] = fb;
+                if (n < lima) mx = fmax(mx, (double)fabsf(fa));
+                if (n < limb) mx = fmax(mx, (double)fabsf(fb));
+            }
         fence_proxy_async_smem();
         __syncthreads();
     }

@@ -234,3 +234,48 @@ def zeldovich_psi(N: int, xmax: float = 5.0, seed: int = 0, a: float = 1.0 / 51.
     phase = (mfdm / c**2 / hbar) * theta
     amp = 1.225 * np.sqrt(np.maximum(RHOC * (1.0 + delta), 0.0) / mfdm_solar)
     return (amp * np.exp(1j * phase)).astype(np.complex128)
+
+
+def zeldovich_psi_device(N: int, xmax: float = 5.0, seed: int = 0, a: float = 1.0 / 51.0, rms_delta: float = 0.02,
+                         mfdm: float = 2.5e-24, slope: float = -2.5, device: int = 0):
+    """The field-level psi of ``zeldovich_psi`` generated on a CUDA device with
+    torch (its own random stream, so not the same field for a given seed), for
+    grids whose host generation would need tens of GB (1024^3).  Returns a
+    complex128 CUDA tensor of shape (N, N, N) in the reference's units."""
+    import torch
+
+    dev = torch.device("cuda", device)
+    box = 2.0 * xmax * 1e3
+    Lg = box / N
+    gen = torch.Generator(device=dev)
+    gen.manual_seed(seed)
+    wk = torch.fft.rfftn(torch.randn((N, N, N), generator=gen, device=dev, dtype=torch.float64))
+    kf = 2.0 * np.pi * torch.fft.fftfreq(N, d=Lg, device=dev, dtype=torch.float64)
+    kr = 2.0 * np.pi * torch.fft.rfftfreq(N, d=Lg, device=dev, dtype=torch.float64)
+    k2 = kf[:, None, None] ** 2 + kf[None, :, None] ** 2 + kr[None, None, :] ** 2
+    k2[0, 0, 0] = 1.0
+    wk *= k2 ** (slope / 4.0)
+    wk[0, 0, 0] = 0.0
+    delta = torch.fft.irfftn(wk, s=(N, N, N))
+    scale = rms_delta / float(delta.std())
+    delta *= scale
+    wk *= -scale / k2
+    del k2
+    pot = torch.fft.irfftn(wk, s=(N, N, N))
+    del wk
+    E = np.sqrt(OMEGA_M0 / a**3 + 1.0 - OMEGA_M0)
+    f = (OMEGA_M0 / a**3 / E**2) ** 0.55
+    vfac = np.sqrt(a) * 100.0 * E * f / 1000.0
+    m2Mpc, s2Myr = 3.086e22, 60.0 * 60.0 * 24.0 * 365.0 * 1e6
+    uc = 1e3 / m2Mpc * s2Myr
+    hbar = 6.58211928e-16 / s2Myr
+    c = 2.99792458e8 / m2Mpc * s2Myr
+    mfdm_solar = mfdm * 1.783e-36 / 1.989e30
+    pot *= (mfdm / c**2 / hbar) * a**1.5 * uc * vfac / (1000.0 * H_LITTLE)  # the phase
+    delta += 1.0
+    delta.clamp_(min=0.0)
+    delta *= RHOC / mfdm_solar
+    amp = delta.sqrt_().mul_(1.225)
+    psi = torch.polar(amp, pot)
+    del amp, pot
+    return psi

@@ -96,7 +96,10 @@ int ifdm_params_from_argv(int argc, char **argv, ifdm_params *p);
 int ifdm_create(const ifdm_params *p, ifdm_ctx **out);
 void ifdm_destroy(ifdm_ctx *ctx);
 const char *ifdm_last_error(const ifdm_ctx *ctx);
-/* 1 if `res` has a compiled FFT plan for `precision`. */
+/* 1 if `res` has a compiled FFT plan for `precision`: 16, 32, 48, 64, 96,
+ * 128, 256, 512 and 1024 (the reference's production grid, job.sh:24) in
+ * IFDM_FP64 and IFDM_FP32; IFDM_MIXED up to 512.  ifdm_load_ic deposits at most
+ * 2^28 particles (512^3); larger boxes start from ifdm_set_psi or a snapshot. */
 int ifdm_supported_res(int res, int precision);
 
 /* Gadget_IC_Generator (src/gadget_IC.h:686-707): read <icpath>.0..3, CIC

@@ -56,6 +56,9 @@ def test_cli_wrong_argc_prints_reference_message():
     assert r.stdout.strip() == "ERROR: Arguments 3!= 11"
 
 
-@pytest.mark.parametrize("n,ok", [(16, 1), (48, 1), (96, 1), (512, 1), (20, 0), (1024, 0)])
-def test_supported_sizes(n, ok):
-    assert ifdm.load_library().ifdm_supported_res(n, 0) == ok
+@pytest.mark.parametrize("n,prec,ok", [(16, 0, 1), (48, 0, 1), (96, 0, 1), (512, 0, 1), (20, 0, 0), (1024, 0, 1),
+                                       (1024, 1, 1), (1024, 2, 0), (512, 2, 1), (2048, 0, 0), (480, 0, 0)])
+def test_supported_sizes(n, prec, ok):
+    """Compiled plans: 16 ... 1024 (the reference's production grid); the mixed
+    mode stops at 512, where its FP64 exchange tiles still fit shared memory."""
+    assert ifdm.load_library().ifdm_supported_res(n, prec) == ok

@@ -176,6 +176,33 @@ template <int DIR, int TN> __device__ __forceinline__ float2 twmul(float2 a, con
     return make_float2(fmaf(a.x, h.x, fmaf(-a.y, hy, cr)), fmaf(a.x, hy, fmaf(a.y, h.x, ci)));
 }
 
+// The same table staged in shared memory by a persistent kernel (one copy per
+// CTA, read with shared-memory loads): the chain then needs no registers to
+// hide global-load latency of its twiddles (a two-transform chain with global
+// twiddles spills at 64 registers, with staged twiddles it does not).
+template <typename C> struct SmemTw {
+    const C *p;
+};
+template <int DIR, int TN> __device__ __forceinline__ double2 twmul(double2 a, SmemTw<double2> tw, int m) {
+    const double2 w = tw.p[m];
+    return cmul(a, DIR < 0 ? w : cconj(w));
+}
+template <int DIR, int TN> __device__ __forceinline__ float2 twmul(float2 a, SmemTw<float2> tw, int m) {
+    const float4 q = reinterpret_cast<const float4 *>(tw.p)[m];
+    const float2 h = make_float2(q.x, q.y), r = make_float2(q.z, q.w);
+    const float hy = DIR < 0 ? h.y : -h.y, ry = DIR < 0 ? r.y : -r.y;
+    const float cr = fmaf(a.x, r.x, -a.y * ry), ci = fmaf(a.x, ry, a.y * r.x);
+    return make_float2(fmaf(a.x, h.x, fmaf(-a.y, hy, cr)), fmaf(a.x, hy, fmaf(a.y, h.x, ci)));
+}
+// bytes of a twiddle table of length N (FP32 tables pair each entry with its remainder)
+template <typename C> __host__ __device__ constexpr size_t tw_bytes(int n) { return size_t(n) * 16; }
+// Copy a table into shared memory (all threads of the block; caller syncs).
+template <typename C> __device__ __forceinline__ void stage_twiddles(C *dst, const C *__restrict__ src, int n) {
+    const float4 *s = reinterpret_cast<const float4 *>(src);
+    float4 *d = reinterpret_cast<float4 *>(dst);
+    for (int i = threadIdx.x; i < n; i += blockDim.x) d[i] = __ldg(s + i);
+}
+
 // One Stockham stage: radix RAD, NS = product of the previous radices.
 template <typename C, int N, int E, int DIR, int L, int LP, int RAD, int NS>
 __device__ __forceinline__ void stockham_stage(C *sm, const C *__restrict__ tw, int l, int t, bool active) {
@@ -281,8 +308,8 @@ __device__ __forceinline__ void stage_load(const SrcT *src, C *v, int l, int t) 
         }
 }
 
-template <typename C, int N, int E, int DIR, int RAD, int NS>
-__device__ __forceinline__ void stage_compute(C *v, const C *__restrict__ tw, int t) {
+template <typename C, int N, int E, int DIR, int RAD, int NS, typename TW>
+__device__ __forceinline__ void stage_compute(C *v, TW tw, int t) {
     constexpr int T = N / E, NB = E / RAD, TWSTEP = N / (NS * RAD);
 #pragma unroll
     for (int b = 0; b < NB; ++b) {
@@ -311,7 +338,7 @@ __device__ __forceinline__ void stage_store(C *dst, const C *v, int l, int t) {
 // through `work` (barrier, store, barrier, load) then compute stage S.
 template <typename C, int N, int E, int DIR, int L, int LP, int S, int NS, int SW = 0>
 struct RegChain {
-    __device__ __forceinline__ static void run(C *work, C *v, const C *__restrict__ tw, int l, int t, bool active) {
+    template <typename TW> __device__ __forceinline__ static void run(C *work, C *v, TW tw, int l, int t, bool active) {
         if constexpr (S < Plan<N>::NST) {
             constexpr int RP = Plan<N>::R[S - 1];
             constexpr int RAD = Plan<N>::R[S];
@@ -330,9 +357,8 @@ struct RegChain {
 // Full transform: stage 0 reads `src` (any element type), later stages go
 // through `work`; on return v holds the outputs, v[b*R + r] = element
 // j + r*N/R (R the last radix, j = t + T*b).  `src` may alias `work`.
-template <typename C, int N, int E, int DIR, int L, int LP, typename SrcT>
-__device__ __forceinline__ void fft_regs(const SrcT *src, C *work, C *v, const C *__restrict__ tw, int l, int t,
-                                         bool active) {
+template <typename C, int N, int E, int DIR, int L, int LP, typename SrcT, typename TW>
+__device__ __forceinline__ void fft_regs(const SrcT *src, C *work, C *v, TW tw, int l, int t, bool active) {
     constexpr int R0 = Plan<N>::R[0];
     if (active) {
         stage_load<C, N, E, L, LP, R0>(src, v, l, t);
@@ -343,8 +369,8 @@ __device__ __forceinline__ void fft_regs(const SrcT *src, C *work, C *v, const C
 
 // Second transform straight from the registers of a first one (requires the
 // plan's first and last radix to be equal).
-template <typename C, int N, int E, int DIR, int L, int LP, int SW = 0>
-__device__ __forceinline__ void fft_regs_chained(C *work, C *v, const C *__restrict__ tw, int l, int t, bool active) {
+template <typename C, int N, int E, int DIR, int L, int LP, int SW = 0, typename TW>
+__device__ __forceinline__ void fft_regs_chained(C *work, C *v, TW tw, int l, int t, bool active) {
     constexpr int R0 = Plan<N>::R[0];
     static_assert(Plan<N>::R[0] == Plan<N>::R[Plan<N>::NST - 1], "chained transform needs equal first/last radix");
     if (active) stage_compute<C, N, E, DIR, R0, 1>(v, tw, t);

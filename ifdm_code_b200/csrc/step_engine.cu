@@ -144,9 +144,10 @@ template <typename R_, typename K_, int N> struct Box {
     // depth and resident blocks per SM of P1, P5 and P9
     static constexpr bool kZT = N >= 256 && std::is_same<R, float>::value && std::is_same<K, float>::value;
     static constexpr int ZST1 = 2, ZST5 = 3, ZST9 = 3, ZB1 = N >= 1024 ? 1 : 2, ZB5 = ZB1, ZB9 = ZB1;
-    static constexpr size_t ZSM1 = kZT ? ZST1 * ZT<(kZT ? N : 256)>::SLOT1 + 64 : 0;
-    static constexpr size_t ZSM5 = kZT ? ZST5 * ZT<(kZT ? N : 256)>::SLOT5 + 64 : 0;
-    static constexpr size_t ZSM9 = kZT ? ZST9 * ZT<(kZT ? N : 256)>::SLOT9 + 64 : 0;
+    // ring slots, the mbarriers (64 bytes) and the staged twiddle table
+    static constexpr size_t ZSM1 = kZT ? ZST1 * ZT<(kZT ? N : 256)>::SLOT1 + 64 + tw_bytes<C>(N) : 0;
+    static constexpr size_t ZSM5 = kZT ? ZST5 * ZT<(kZT ? N : 256)>::SLOT5 + 64 + tw_bytes<C>(N) : 0;
+    static constexpr size_t ZSM9 = kZT ? ZST9 * ZT<(kZT ? N : 256)>::SLOT9 + 64 + tw_bytes<C>(N) : 0;
     static inline int zt1grid = 0, zt5grid = 0, zt9grid = 0;  // persistent grids of the bulk-copy z passes
     using TT = TmaTile<R, K, N, 1>;
     using TX = TmaTile<R, K, N, 2>;

@@ -64,9 +64,12 @@ template <typename R, typename K, int N, int AXIS = 1> struct TmaTile {
     static constexpr bool OWN_WORK = SPLIT;
     static constexpr int LPW = L;
     static constexpr size_t WORK_BYTES = OWN_WORK ? size_t(N) * LPW * sizeof(C) : 0;
-    static constexpr size_t SMEM = STAGES * TILE_BYTES + WORK_BYTES + 64;
+    // the N-point twiddle table, staged in shared memory once per CTA
+    static constexpr size_t TWOFF = STAGES * TILE_BYTES + WORK_BYTES + 64;
+    static constexpr size_t SMEM = TWOFF + tw_bytes<C>(N);
     static_assert(NT <= 1024, "block size");
     static_assert(SMEM <= 227 * 1024, "shared memory per block");
+    static_assert(TWOFF % 16 == 0, "twiddle table alignment");
 };
 
 template <typename R, typename K, int N, int AXIS, int MODE, int DIR>
@@ -89,6 +92,9 @@ __global__ void __launch_bounds__(TmaTile<R, K, N, AXIS>::NT, TmaTile<R, K, N, A
         mbar_init_fence();
         prefetch_tmap(&map);
     }
+    C *stw = reinterpret_cast<C *>(smraw + TL::TWOFF);
+    stage_twiddles(stw, tw, N);
+    const SmemTw<C> tws{stw};
     __syncthreads();
     const int my_n = blockIdx.x < (unsigned)ntiles ? (ntiles - 1 - (int)blockIdx.x) / (int)gridDim.x + 1 : 0;
     auto issue = [&](int i) {
@@ -131,8 +137,8 @@ __global__ void __launch_bounds__(TmaTile<R, K, N, AXIS>::NT, TmaTile<R, K, N, A
         // stage 0 straight from the landing slot
         stage_load<C, N, E, L, L, R0>(land, v, l, t);
         if constexpr (TL::OWN_WORK) fence_proxy_async_smem();  // slot is released at the next barrier
-        stage_compute<C, N, E, (MODE == 0 ? DIR : -1), R0, 1>(v, tw, t);
-        RegChain<C, N, E, (MODE == 0 ? DIR : -1), L, LPW, 1, R0, TL::SWZ>::run(wk, v, tw, l, t, true);
+        stage_compute<C, N, E, (MODE == 0 ? DIR : -1), R0, 1>(v, tws, t);
+        RegChain<C, N, E, (MODE == 0 ? DIR : -1), L, LPW, 1, R0, TL::SWZ>::run(wk, v, tws, l, t, true);
         if (MODE != 0) {
             // v[b*RL + r] holds element n = (t + T*b) + r*N/RL of the forward transform
             if (MODE == 1) {
@@ -165,7 +171,7 @@ __global__ void __launch_bounds__(TmaTile<R, K, N, AXIS>::NT, TmaTile<R, K, N, A
                         v[b * RL + r] = cscale(v[b * RL + r], k2 == 0 ? K(0) : K(-1) / K(k2));
                     }
             }
-            fft_regs_chained<C, N, E, +1, L, LPW, TL::SWZ>(wk, v, tw, l, t, true);
+            fft_regs_chained<C, N, E, +1, L, LPW, TL::SWZ>(wk, v, tws, l, t, true);
         }
         if ((g % W) < VW) {
             const size_t b0 = AXIS == 1 ? size_t(g / W) * N * W + size_t(g % W) : size_t(g);

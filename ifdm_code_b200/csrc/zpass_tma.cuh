@@ -9,7 +9,8 @@
 // stage reads element n of row l with the row index fastest across a warp,
 // and the pad puts those rows in different banks.  Later stages exchange
 // through the same slot laid out [n][l] (the swizzled 8-line tile of the
-// narrow x passes).  Every mbarrier wait is bounded (error bit in TState).
+// narrow x passes).  The twiddle table is staged in shared memory once per
+// CTA.  Every mbarrier wait is bounded (error bit in TState).
 //
 //   k_kick_fft_z_tma      P1: kick with the merged coefficients, remove the
 //                         offset c, forward FFT along z.
@@ -98,6 +99,9 @@ __global__ void __launch_bounds__(ZT<N>::NT, MINB)
     extern __shared__ __align__(128) unsigned char smraw[];
     uint64_t *bar = reinterpret_cast<uint64_t *>(smraw + ST * Z::SLOT1);
     const int tid = threadIdx.x, l = tid % L, t = tid / L;
+    C *stw = reinterpret_cast<C *>(smraw + ST * Z::SLOT1 + 64);
+    stage_twiddles(stw, tw, N);
+    const SmemTw<C> tws{stw};
     ring_init<ST>(bar);
     const int my_n = ztiles_of_block(ntiles);
     auto issue = [&](int i) {
@@ -132,8 +136,8 @@ __global__ void __launch_bounds__(ZT<N>::NT, MINB)
                 const double p = cp * (double)lf[n] + cq * (double)cnorm2(g) + alpha;
                 v[b * R0 + r] = cmul(g, expmi<float>(p)) - c0;
             }
-        stage_compute<C, N, E, -1, R0, 1>(v, tw, t);
-        RegChain<C, N, E, -1, L, L, 1, R0, 1>::run(reinterpret_cast<C *>(slot), v, tw, l, t, true);
+        stage_compute<C, N, E, -1, R0, 1>(v, tws, t);
+        RegChain<C, N, E, -1, L, L, 1, R0, 1>::run(reinterpret_cast<C *>(slot), v, tws, l, t, true);
         C *out = psi + (size_t(blockIdx.x + (long)i * gridDim.x) * L + l) * N;
 #pragma unroll
         for (int b = 0; b < E / RL; ++b)
@@ -157,6 +161,9 @@ __global__ void __launch_bounds__(ZT<N>::NT, MINB)
     extern __shared__ __align__(128) unsigned char smraw[];
     uint64_t *bar = reinterpret_cast<uint64_t *>(smraw + ST * Z::SLOT5);
     const int tid = threadIdx.x, l = tid % L, t = tid / L;
+    C *stw = reinterpret_cast<C *>(smraw + ST * Z::SLOT5 + 64);
+    stage_twiddles(stw, tw, N);
+    const SmemTw<C> tws{stw};
     // the density transform: 4 lines, T threads each (whole warps: threads < LH * T)
     const bool act = tid < LH * T;
     const int p = tid % LH, tq = tid / LH;
@@ -189,8 +196,8 @@ __global__ void __launch_bounds__(ZT<N>::NT, MINB)
         for (int b = 0; b < E / R0; ++b)
 #pragma unroll
             for (int r = 0; r < R0; ++r) v[b * R0 + r] = lp[t + T * b + r * (N / R0)];
-        stage_compute<C, N, E, +1, R0, 1>(v, tw, t);
-        RegChain<C, N, E, +1, L, L, 1, R0, 1>::run(wk, v, tw, l, t, true);
+        stage_compute<C, N, E, +1, R0, 1>(v, tws, t);
+        RegChain<C, N, E, +1, L, L, 1, R0, 1>::run(wk, v, tws, l, t, true);
         // psi = IFFT + c; rho = |psi|^2 - mu into a float tile that pairs rows
         // p and p+4 of element n: rt[(n*LH + p)*2 + h] holds row p + h*LH
         // (conflict-free stores of the [l, t] layout and float2 loads of the
@@ -222,9 +229,9 @@ __global__ void __launch_bounds__(ZT<N>::NT, MINB)
             for (int b = 0; b < E / R0; ++b)
 #pragma unroll
                 for (int r = 0; r < R0; ++r) v[b * R0 + r] = rp[(tq + T * b + r * (N / R0)) * LH + p];
-            stage_compute<C, N, E, -1, R0, 1>(v, tw, tq);
+            stage_compute<C, N, E, -1, R0, 1>(v, tws, tq);
         }
-        RegChain<C, N, E, -1, LH, LH, 1, R0, 3>::run(wk, v, tw, p, tq, act);
+        RegChain<C, N, E, -1, LH, LH, 1, R0, 3>::run(wk, v, tws, p, tq, act);
         // Z_k in an [k][p] tile, then the two half spectra of each line
         __syncthreads();
         if (act) {
@@ -262,6 +269,9 @@ __global__ void __launch_bounds__(ZT<N>::NT, MINB)
     extern __shared__ __align__(128) unsigned char smraw[];
     uint64_t *bar = reinterpret_cast<uint64_t *>(smraw + ST * Z::SLOT9);
     const int tid = threadIdx.x, l = tid % L, t = tid / L;
+    C *stw = reinterpret_cast<C *>(smraw + ST * Z::SLOT9 + 64);
+    stage_twiddles(stw, tw, N);
+    const SmemTw<C> tws{stw};
     ring_init<ST>(bar);
     const int my_n = ztiles_of_block(ntiles);
     auto issue = [&](int i) {
@@ -297,8 +307,8 @@ __global__ void __launch_bounds__(ZT<N>::NT, MINB)
                 }
                 v[bb * R0 + r] = n <= M ? mkc(a.x - b.y, a.y + b.x) : mkc(a.x + b.y, b.x - a.y);
             }
-        stage_compute<C, N, E, +1, R0, 1>(v, tw, t);
-        RegChain<C, N, E, +1, L, L, 1, R0, 1>::run(reinterpret_cast<C *>(slot), v, tw, l, t, true);
+        stage_compute<C, N, E, +1, R0, 1>(v, tws, t);
+        RegChain<C, N, E, +1, L, L, 1, R0, 1>::run(reinterpret_cast<C *>(slot), v, tws, l, t, true);
         const long ra = long(blockIdx.x + (long)i * gridDim.x) * ROWS + l, rb = ra + L;
         // elements of rows below win_rows, and the first win_tail of row win_rows, are in the window
         const int lima = ra < win_rows ? N : (ra == win_rows ? win_tail : 0);

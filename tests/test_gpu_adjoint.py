@@ -125,7 +125,7 @@ def test_adjoint_128_200_steps_mixed():
     _fd_check(n, nsteps, C, ckpt, "mixed", 5e-3, ndir=16)
 
 
-@pytest.mark.parametrize("prec,tol", [("fp64", 2e-5), ("mixed", 2e-3), ("fp32", 5e-3)])
+@pytest.mark.parametrize("prec,tol", [("fp64", 2e-5), ("mixed", 2e-3), ("fp32", 1e-2)])
 def test_adjoint_with_self_interaction_matches_finite_differences(prec, tol):
     """The linearised g|psi|^2 term of the kick: g set so that the densest
     cell turns by 0.1 rad in the first step (the self-interaction strength of

@@ -28,7 +28,7 @@ EXPORTS = [
     "ifdm_supported_res", "ifdm_load_ic", "ifdm_load_snapshot", "ifdm_set_psi", "ifdm_get_psi", "ifdm_get_phi",
     "ifdm_get_state", "ifdm_power_spectrum", "ifdm_get_energies", "ifdm_run", "ifdm_step", "ifdm_write_snapshot", "ifdm_write_snapshot_async",
     "ifdm_flush_snapshots", "ifdm_set_snapshot_streaming", "ifdm_snapshots_written", "ifdm_synchronize", "ifdm_stream",
-    "ifdm_profile_passes", "ifdm_pass_bytes", "ifdm_fft3d", "ifdm_poisson_static", "ifdm_record_steps",
+    "ifdm_profile_passes", "ifdm_pass_bytes", "ifdm_fft3d", "ifdm_fft_slab", "ifdm_poisson_static", "ifdm_record_steps",
     "ifdm_adjoint", "ifdm_batch_create", "ifdm_batch_step", "ifdm_batch_tune", "ifdm_batch_get_tuning",
     "ifdm_batch_set_tuning", "ifdm_batch_synchronize", "ifdm_batch_record_steps", "ifdm_batch_adjoint", "ifdm_batch_info", "ifdm_batch_last_error",
     "ifdm_batch_destroy",
@@ -114,6 +114,8 @@ def load_library() -> C.CDLL:
     lib.ifdm_profile_passes.argtypes = [P, C.c_int, C.c_double, D, C.POINTER(C.c_char_p), C.c_int]
     lib.ifdm_pass_bytes.argtypes = [P, D, C.c_int]
     lib.ifdm_fft3d.argtypes = [C.c_void_p, C.c_int, C.c_int, C.c_int, C.c_void_p]
+    lib.ifdm_fft_slab.argtypes = [C.c_void_p, C.c_int, C.c_int, C.c_int, C.c_int, C.c_int, C.c_int, C.c_int,
+                                  C.c_void_p]
     lib.ifdm_poisson_static.argtypes = [C.c_void_p, C.c_void_p, C.c_int, C.c_double, C.c_double, C.c_void_p]
     lib.ifdm_record_steps.argtypes = [P, C.c_int, C.c_double, C.c_int]
     lib.ifdm_adjoint.argtypes = [P, C.c_void_p, C.c_void_p]

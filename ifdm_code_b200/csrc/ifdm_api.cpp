@@ -677,6 +677,16 @@ void ifdm_batch_destroy(ifdm_batch *b) {
     delete b;  // the engine's graphs and buffers do not refer to the stream
 }
 
+int ifdm_fft_slab(void *data, int n, int planes, int axis, int precision, int sign, int op, int y0, void *stream) {
+    if (!data || (sign != 1 && sign != -1) || precision < 0 || precision > 2 || axis < 0 || axis > 2 || planes < 1 ||
+        planes > n || op < 0 || op > 1 || (op == 1 && axis != 0) || y0 < 0 || y0 + planes > n)
+        return IFDM_ERR_ARGS;
+    if (!supported_n(n, precision)) return IFDM_ERR_UNSUPPORTED;
+    const std::string e = fft_slab(data, n, planes, axis, precision, sign, op, y0, (cudaStream_t)stream);
+    if (e.empty()) return IFDM_OK;
+    return e.rfind("planes", 0) == 0 ? IFDM_ERR_ARGS : IFDM_ERR_CUDA;
+}
+
 int ifdm_fft3d(void *data, int n, int precision, int sign, void *stream) {
     if (!data || (sign != 1 && sign != -1) || precision < 0 || precision > 2) return IFDM_ERR_ARGS;
     if (!supported_n(n, precision)) return IFDM_ERR_UNSUPPORTED;

@@ -96,6 +96,7 @@ template <typename R_, typename K_, int N> struct Box {
         CUDA_TRY(prep(k_fft_z<R, K, N, -1>, SMZ));
         CUDA_TRY(prep(k_fft_z<R, K, N, +1>, SMZ));
         CUDA_TRY(prep(k_source_r2c_z<R, K, N>, SMZ));
+        CUDA_TRY(prep(k_fft_x_poisson_slab<R, K, N>, SM));
         int sms = 0;
         CUDA_TRY(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));
         if constexpr (kZPipe) {
@@ -243,6 +244,29 @@ template <typename R_, typename K_, int N> struct Box {
                            const CUtensorMap *tm) {
         k_source_r2c_z<R, K, N><<<zrows(), TZ::NT, SMZ, s>>>(w, rhok, ts_adj, tw, twh);
         for (int p = 6; p <= 9; ++p) pass(p, s, nullptr, pw, rhok, ts_adj, nullptr, tw, twh, 0, 0, tm);
+    }
+
+    // One axis of a slab's local FFT step (plain passes): axis 2 = z on the
+    // x-slab [planes][N][N], axis 1 = y on the x-slab, axis 0 = x on the
+    // transposed y-slab [N][planes][N] (op 1: forward, -1/(kappa^2 N^3) with
+    // global y offset y0, inverse).
+    static std::string fft_slab(G *data, int planes, int axis, int sign, int op, int y0, const C *tw, cudaStream_t s) {
+        const size_t nl = size_t(planes) * N;
+        if (nl % TL::L || nl % TZ::L) return "planes * n must be a multiple of the tile lines";
+        const unsigned gz = unsigned(nl / TZ::L), gl = unsigned(nl / TL::L), nt = TL::NT;
+        if (axis == 2) {
+            if (sign < 0) k_fft_z<R, K, N, -1><<<gz, TZ::NT, SMZ, s>>>(data, tw, 0x2545f491u);
+            else k_fft_z<R, K, N, +1><<<gz, TZ::NT, SMZ, s>>>(data, tw, 0x2545f491u);
+        } else if (axis == 1) {
+            if (sign < 0) k_fft_yx<R, K, N, -1, 1><<<gl, nt, SM, s>>>(data, N, N, nullptr, 0, tw);
+            else k_fft_yx<R, K, N, +1, 1><<<gl, nt, SM, s>>>(data, N, N, nullptr, 0, tw);
+        } else if (op == 1) {
+            k_fft_x_poisson_slab<R, K, N><<<gl, nt, SM, s>>>(data, planes, y0, tw);
+        } else {
+            if (sign < 0) k_fft_yx<R, K, N, -1, 2><<<gl, nt, SM, s>>>(data, planes, planes, nullptr, 0, tw);
+            else k_fft_yx<R, K, N, +1, 2><<<gl, nt, SM, s>>>(data, planes, planes, nullptr, 0, tw);
+        }
+        return "";
     }
 
     static void fft3d(G *data, int sign, const C *tw, cudaStream_t s) {
@@ -871,6 +895,25 @@ std::string StepEngine::adjoint(const double *g_final_dev, double *g0_dev) {
     CUDA_TRY(cudaGetLastError());
     recorded_ = 0;  // the replay consumed the state; record again before another adjoint
     return "";
+}
+
+std::string fft_slab(void *data, int n, int planes, int axis, int precision, int sign, int op, int y0,
+                     cudaStream_t stream) {
+    if (!supported_n(n, precision)) return "unsupported grid size " + std::to_string(n);
+    void *tw = nullptr;
+    std::string e = get_twiddles(n, compute_kind(precision), &tw);
+    if (!e.empty()) return e;
+    return with_box2(n, precision, [&](auto box) -> std::string {
+        using B = decltype(box);
+        using C = typename B::C;
+        using G = typename B::G;
+        std::string e2 = B::configure();
+        if (!e2.empty()) return e2;
+        e2 = B::fft_slab((G *)data, planes, axis, sign, op, y0, (const C *)tw, stream);
+        if (!e2.empty()) return e2;
+        CUDA_TRY(cudaGetLastError());
+        return "";
+    });
 }
 
 std::string fft3d(void *data, int n, int precision, int sign, cudaStream_t stream) {

@@ -136,6 +136,9 @@ class StepEngine {
 
 // Plain in-place 3-D c2c FFT of device data (complex128 if precision 0).
 std::string fft3d(void *data, int n, int precision, int sign, cudaStream_t stream);
+// One axis of a slab-decomposed 3-D FFT on device data (ifdm_fft_slab).
+std::string fft_slab(void *data, int n, int planes, int axis, int precision, int sign, int op, int y0,
+                     cudaStream_t stream);
 bool supported_n(int n);
 // grid sizes with a compiled plan in a precision mode (0 FP64, 1 FP32, 2 mixed)
 bool supported_n(int n, int precision);

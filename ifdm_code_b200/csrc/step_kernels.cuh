@@ -506,6 +506,40 @@ __global__ void __launch_bounds__(Tile<R, K, N>::NT)
             rhok[q + n * S] = Cvt<R, K>::out(sm[n * TL::LP + l], salt, q + n * S);
 }
 
+// x-pass of a slab-decomposed Poisson solve.  The data are a rank's y-slab
+// [x][planes][N] of a complex field already transformed along z and y (the
+// layout after the x <-> y transpose of the slab scheme), holding the global
+// y-planes y0 .. y0 + planes - 1: forward FFT along x, multiply by
+// -1/(kappa^2 N^3) (0 at kappa = 0; the 1/N^3 of the three inverse
+// transforms folded in), inverse FFT along x.
+template <typename R, typename K, int N>
+__global__ void __launch_bounds__(Tile<R, K, N>::NT)
+    k_fft_x_poisson_slab(cx<R> *__restrict__ data, int planes, int y0, const cx<K> *__restrict__ tw) {
+    using TL = Tile<R, K, N>;
+    using C = typename TL::C;
+    extern __shared__ __align__(16) unsigned char smraw[];
+    C *sm = reinterpret_cast<C *>(smraw);
+    const int l = threadIdx.x % TL::L;
+    const long q = long(blockIdx.x) * TL::L + l;  // column = y_local * N + z
+    const int y = y0 + int(q / N), z = int(q % N);
+    const size_t S = size_t(N) * planes;
+    for (int n = threadIdx.x / TL::L; n < N; n += TL::NT / TL::L) sm[n * TL::LP + l] = cin<K>(data[q + n * S]);
+    __syncthreads();
+    fft_tile<C, N, TL::E, -1, TL::L, TL::LP>(sm, tw);
+    const int ky = kappa(y, N), kz = kappa(z, N);
+    const int k2yz = ky * ky + kz * kz;
+    const double inv3 = 1.0 / ((double)N * N * N);
+    for (int n = threadIdx.x / TL::L; n < N; n += TL::NT / TL::L) {
+        const int kx = kappa(n, N);
+        const int k2 = kx * kx + k2yz;
+        sm[n * TL::LP + l] = cscale(sm[n * TL::LP + l], k2 == 0 ? K(0) : K(-inv3 / k2));
+    }
+    __syncthreads();
+    fft_tile<C, N, TL::E, +1, TL::L, TL::LP>(sm, tw);
+    for (int n = threadIdx.x / TL::L; n < N; n += TL::NT / TL::L)
+        data[q + n * S] = Cvt<R, K>::out(sm[n * TL::LP + l], 0x6a09e667u, q + n * S);
+}
+
 // ------------------------------------------------------- state transfer ---
 // out = S * psi_s * exp(-i (cP phi_s + cQ |psi_s|^2)) as complex128; the
 // coefficients are read from the TState field pair selected by `which`

@@ -241,6 +241,19 @@ void ifdm_batch_destroy(ifdm_batch *b);
  * -- the contract of the reference's fftw_mpi_plan_dft_3d plans
  * (src/CosmoBEC_MPI.cpp:176-177). */
 int ifdm_fft3d(void *data, int n, int precision, int sign, void *stream);
+/* One axis of the local step of a slab-decomposed 3-D FFT, in place on device
+ * data: the reference splits the box into x-slabs of local_n0 = n/P planes per
+ * MPI rank (src/struct3D.h:3-15) and its fftw_mpi plans transpose between
+ * ranks (src/CosmoBEC_MPI.cpp:174-177).  Here a rank transforms z and y on
+ * its x-slab [planes][n][n] (axis 2, axis 1) and x on the transposed y-slab
+ * [n][planes][n] (axis 0) that an all-to-all gives it; the transposes are the
+ * caller's (NCCL or gloo, ifdm_code_b200.slab).  op 1 (axis 0 only): forward
+ * FFT along x, multiply by -1/(kappa^2 n^3) with the slab's global y planes
+ * y0 .. y0+planes-1 (0 at kappa = 0), inverse FFT -- the Poisson multiplier of
+ * src/CosmoBEC_MPI.cpp:80-119 with the three inverse normalisations folded in;
+ * sign is then ignored.  planes * n must be a multiple of 16; bad arguments
+ * return IFDM_ERR_ARGS. */
+int ifdm_fft_slab(void *data, int n, int planes, int axis, int precision, int sign, int op, int y0, void *stream);
 
 /* Gravitational potential of a wave function without allocating any device
  * memory.  No counterpart in the reference: it exists for callers that cannot

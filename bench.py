@@ -800,7 +800,11 @@ def run_reference(args):
         "vs_baseline": None, "dtype": "f64", "data": "synthetic",
         "config": {"workload": f"{N}^3 leap-frog step (reference loop, rerun from a synthetic snapshot), "
                                f"g={G:.4e} eV cm^3 ({args.g_phase} rad/step at the densest cell)",
-                   "res": N, "g_eV_cm3": G},
+                   "res": N, "g_eV_cm3": G,
+                   "steps_cap": f"at most --ref-max-steps={args.ref_max_steps} timed steps: one reference step "
+                                f"takes ~13 s at 512^3 on this host, so the arm stays within a few minutes",
+                   "reference_build": "the reference's MPI-FFTW build is unavailable on this box (no MPI, FFTW3 "
+                                      "or GSL); its own sources run against single-rank shims"},
         "cpu_baseline": {"value": value, "unit": "cell-steps/s", "cores": cores, "kind": "reference",
                          "sample": f"{len(dts)} timed steps after {W} warm-up at {N}^3; FFTs on {cores} OpenMP "
                                    "threads (shim), pointwise loops on 1 thread as one MPI rank runs them"},
@@ -880,7 +884,7 @@ def main():
                     help="snapshots per schedule of the blocking vs streamed timing (0 skips it)")
     ap.add_argument("--precision-steps", type=int, default=1000,
                     help="steps of the precision gate (density error vs FP64); 0 skips it")
-    ap.add_argument("--ref-max-steps", type=int, default=3,
+    ap.add_argument("--ref-max-steps", type=int, default=6,
                     help="bound on timed reference steps (each is ~tens of seconds at 512^3)")
     args = ap.parse_args()
     if args.warmup < 3 and args.impl == "ours":

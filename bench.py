@@ -644,6 +644,21 @@ def run_ours(args):
     }
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         out["cpu_baseline"] = cpu_baseline_port(N, psi0, C)
+    # the figures the metric names, last on the line (readers that keep its tail see them)
+    gates = {}
+    if prec_report:
+        gates["512_g001_fp32"] = prec_report["fp32"]["density_relL2"]
+        gates["512_g001_mixed"] = prec_report["mixed"]["density_relL2"]
+    for key, rep in (("256_g0", prec256), ("256_g01", prec256g)):
+        if rep:
+            gates[key + "_fp32"] = rep["fp32"]["density_relL2"]
+            gates[key + "_mixed"] = rep["mixed"]["density_relL2"]
+    out["summary"] = {"ms_per_step": {p: round(res[p]["ms"] / K, 4) for p in res},
+                      "fp32_over_fp64": round(vals["fp32"] / fp64_value, 4),
+                      "density_relL2_after_1000_steps": {k: float("%.3g" % v) for k, v in gates.items()},
+                      "gate": gate, "headline_path": head,
+                      "adjoint_over_forward": round(adj["adjoint_over_forward"], 3) if adj else None,
+                      "e2e_over_value": round(e2e_value / value, 3)}
     rep_.close()
     if rank == 0:
         print(json.dumps(out))

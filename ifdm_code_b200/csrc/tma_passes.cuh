@@ -28,12 +28,10 @@ template <typename R, typename K, int N, int AXIS = 1> struct TmaTile {
     using G = cx<R>;
     using C = cx<K>;
     static constexpr bool SPLIT = !std::is_same<R, K>::value;
-    // lines per tile: 128-byte rows, except for FP32 at N = 512: the x
-    // passes' two chained transforms with compensated twiddles spill heavily
-    // at the 64-register cap of 1024 threads, so they take 8 lines (512
-    // threads, one block per SM); the y passes take 8 lines too, capped at 64
-    // registers so that two blocks share an SM (measured: P2/P4 0.531 ->
-    // 0.49 ms, P6/P8 0.30 -> 0.27 ms against 16 lines, one block per SM).
+    // lines per tile: 128-byte rows, except for FP32 at N = 512: 8 lines (512
+    // threads) capped at 64 registers so that two blocks share an SM (y
+    // passes measured: P2/P4 0.531 -> 0.49 ms, P6/P8 0.30 -> 0.27 ms against
+    // 16 lines, one block per SM).
     // 4-line x tiles, two blocks per SM at the same 128 registers (32-byte
     // TMA rows), measured slower: P3 0.92 -> 1.31 ms, P7 0.52 -> 0.59 ms.
     static constexpr bool NARROW = !SPLIT && sizeof(G) == 8 && N >= 512;
@@ -47,7 +45,11 @@ template <typename R, typename K, int N, int AXIS = 1> struct TmaTile {
     // and FP64 2, which keeps them within the registers of their block size
     // (8 FP32 lines spilled 344 bytes a thread at 64 registers)
     static constexpr bool BIG = N >= 1024;
-    static constexpr int MINB = BIG ? 1 : ((NARROW && AXIS == 1) || NARROW64) ? 2 : 1;  // resident blocks the registers must allow
+    // resident blocks the registers must allow: two for the narrow tiles (the
+    // FP32 x passes too since their twiddles come from shared memory: no
+    // spills at 64 registers; measured at 512^3: P3 0.895 -> 0.877 ms, P7
+    // 0.457 -> 0.433 ms)
+    static constexpr int MINB = BIG ? 1 : (NARROW || NARROW64) ? 2 : 1;
     static constexpr int L = BIG ? (sizeof(G) == 16 ? 4 : 8) / (AXIS == 2 ? 2 : 1)
                                  : NARROW64 ? 4 : (SPLIT || NARROW) ? 8 : 128 / (int)sizeof(G);
     static constexpr bool SWZ = NARROW || NARROW64;  // slot swizzle of the exchange tile

@@ -156,8 +156,9 @@ def test_adjoint_differentiation_config_fp32():
     central differences and against the FP64 adjoint.
 
     The configuration's own schedule (the step scale that reaches a = 0.5 in
-    200 steps, 0.22) hands some steps to the potential criterion, whose step
-    size depends on max|phi| and is not differentiated; the test uses the
+    200 steps, 0.22) hands its last steps to the potential criterion (from
+    step 193 on with this IC), whose step size depends on max|phi| and is not
+    differentiated; the test uses the
     largest scale of a fixed ladder at which all 200 steps stay kinetic-limited
     and prints where the larger ones leave it."""
     n, nsteps, ckpt = 128, 200, 20
@@ -169,13 +170,13 @@ def test_adjoint_differentiation_config_fp32():
             C = c
             break
     assert C is not None
-    worst = _fd_check(n, nsteps, C, ckpt, "fp32", 2e-2, ndir=16)
+    worst = _fd_check(n, nsteps, C, ckpt, "fp32", 2e-3, ndir=16)  # measured worst 2.6e-4
     target = _target(n, nsteps, C, "fp64")
     _, g64 = _gradient(n, nsteps, C, ckpt, "fp64", target)
     _, g32 = _gradient(n, nsteps, C, ckpt, "fp32", target)
     e = float((g32 - g64).abs().norm() / g64.abs().norm())
     print(f"128^3/200 steps, C={C}: fp32 adjoint vs FD worst {worst:.2e}, vs FP64 adjoint {e:.2e}")
-    assert e <= 2e-2
+    assert e <= 5e-4  # measured 3.6e-5
 
 
 def test_reduced_precision_adjoint_close_to_fp64():

@@ -32,8 +32,9 @@ pytestmark = pytest.mark.gpu
 N = 512
 STEPS = 2
 PSI_TOL = 1e-10  # FP64 drop-in bar
-# reduced precision after two steps: psi relative L2 (phase errors included)
-REDUCED_TOL = {"fp32": 2e-5, "mixed": 2e-6}
+# reduced precision after two steps: psi relative L2 (phase errors included);
+# measured on a B200: FP32 8.3e-8, mixed 6.4e-8 (FP64: 4.6e-16)
+REDUCED_TOL = {"fp32": 1e-6, "mixed": 5e-7}
 
 
 @pytest.fixture(scope="module")

@@ -84,4 +84,4 @@ def test_steps_1024(monkeypatch):
     d32 = _rel(out["fp32"].abs() ** 2, out["fp64"].abs() ** 2)
     print(f"1024^3, 2 steps: fp64 tma vs plain {e_tma:.2e}; fp32 vs fp64 psi {e32:.2e}, density {d32:.2e}")
     assert e_tma <= 1e-13
-    assert e32 <= 2e-5 and d32 <= 5e-6
+    assert e32 <= 1e-6 and d32 <= 1e-6  # measured: 8.0e-8, 1.1e-7 (TMA vs plain 8.9e-17)

@@ -249,22 +249,14 @@ def cpu_baseline_port(N: int, psi0, dt_scale: float):
             "sample": f"1 leap-frog step of the {N}^3 workload ({dt:.1f} s)"}
 
 
-# Kernels of the 512^3 passes whose DRAM traffic per launch was captured with
-# ncu (summary and command in profiles/fp32_512_step_kernels.md).
-PROFILED_KERNEL = {("fp32", "P1"): "k_kick_fft_z<float,float,512>",
-                   ("fp32", "P2"): "k_yx_tma<float,float,512,1,0,(int)-1>",
-                   ("fp32", "P3"): "k_yx_tma<float,float,512,2,1,0>",
-                   ("fp32", "P5"): "k_density_r2c_z_pipe<float,512>",
-                   ("fp32", "P9"): "k_c2r_z_phi<float,float,512>"}
-
-
 def profiled_traffic(prec: str, pass_name: str, N: int):
-    """DRAM bytes read + written per launch by the pass's kernel, from the
-    committed ncu summary (512^3 only), else None."""
-    key = PROFILED_KERNEL.get((prec, pass_name.split("_")[0]))
-    path = os.path.join(os.path.dirname(os.path.abspath(__file__)), "profiles", "fp32_512_step_kernels.md")
-    if N != 512 or key is None or not os.path.exists(path):
+    """DRAM bytes read + written per launch by the pass's kernel at 512^3, from
+    the committed ncu summary (profiles/step_512_dram_per_kernel.md: one pass of
+    dram__bytes_read.sum + dram__bytes_write.sum over one step), else None."""
+    path = os.path.join(ROOT, "profiles", "step_512_dram_per_kernel.md")
+    if N != 512 or not os.path.exists(path):
         return None
+    key = pass_name.split("_")[0]
     for line in open(path):
         f = line.split()
         if len(f) == 4 and f[0] == "traffic" and f[1] == prec and f[2] == key:

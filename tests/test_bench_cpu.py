@@ -58,4 +58,6 @@ def test_profiled_traffic_lookup(bench):
     t = bench.profiled_traffic("fp32", "P5_ifft_z_density_r2c_z", 512)
     assert t is not None and 1e9 < t < 1e10
     assert bench.profiled_traffic("fp32", "P5_ifft_z_density_r2c_z", 256) is None
-    assert bench.profiled_traffic("fp64", "P5_ifft_z_density_r2c_z", 512) is None
+    t64 = bench.profiled_traffic("fp64", "P5_ifft_z_density_r2c_z", 512)
+    assert t64 is not None and 1.5 * t < t64 < 2.5 * t  # FP64 moves twice the bytes
+    assert bench.profiled_traffic("fp64", "P5_ifft_z_density_r2c_z", 1024) is None

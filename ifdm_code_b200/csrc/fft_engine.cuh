@@ -367,6 +367,80 @@ __device__ __forceinline__ void fft_regs(const SrcT *src, C *work, C *v, TW tw, 
     RegChain<C, N, E, DIR, L, LP, 1, R0>::run(work, v, tw, l, t, active);
 }
 
+// ------------------------------------------- two lines per thread (FP32) --
+// Thread (lp, t) of an FP32 tile [n][L] owns element n of lines 2lp and
+// 2lp + 1, which share one 16-byte word: each exchange moves the pair with
+// one 128-bit shared-memory access and each twiddle load serves both lines
+// (half the shared-memory instructions and twiddle wavefronts of one line per
+// thread).  va holds line 2lp, vb line 2lp + 1, in the RegChain order.
+template <int DIR> __device__ __forceinline__ void twmul_pair(float2 &a, float2 &b, SmemTw<float2> tw, int m) {
+    const float4 q = reinterpret_cast<const float4 *>(tw.p)[m];
+    const float hy = DIR < 0 ? q.y : -q.y, ry = DIR < 0 ? q.w : -q.w;
+    float cr = fmaf(a.x, q.z, -a.y * ry), ci = fmaf(a.x, ry, a.y * q.z);
+    a = make_float2(fmaf(a.x, q.x, fmaf(-a.y, hy, cr)), fmaf(a.x, hy, fmaf(a.y, q.x, ci)));
+    cr = fmaf(b.x, q.z, -b.y * ry);
+    ci = fmaf(b.x, ry, b.y * q.z);
+    b = make_float2(fmaf(b.x, q.x, fmaf(-b.y, hy, cr)), fmaf(b.x, hy, fmaf(b.y, q.x, ci)));
+}
+
+template <int N, int E, int LH, int RAD, int SW = 0>
+__device__ __forceinline__ void stage_load_pair(const float4 *src, float2 *va, float2 *vb, int lp, int t) {
+    constexpr int T = N / E, NB = E / RAD, STRIDE = N / RAD;
+#pragma unroll
+    for (int b = 0; b < NB; ++b)
+#pragma unroll
+        for (int r = 0; r < RAD; ++r) {
+            const float4 q = src[slot<SW>(t + T * b + r * STRIDE) * LH + lp];
+            va[b * RAD + r] = make_float2(q.x, q.y);
+            vb[b * RAD + r] = make_float2(q.z, q.w);
+        }
+}
+
+template <int N, int E, int DIR, int RAD, int NS>
+__device__ __forceinline__ void stage_compute_pair(float2 *va, float2 *vb, SmemTw<float2> tw, int t) {
+    constexpr int T = N / E, NB = E / RAD, TWSTEP = N / (NS * RAD);
+#pragma unroll
+    for (int b = 0; b < NB; ++b) {
+        const int k = (t + T * b) % NS;
+        if (NS > 1) {
+#pragma unroll
+            for (int r = 1; r < RAD; ++r) twmul_pair<DIR>(va[b * RAD + r], vb[b * RAD + r], tw, k * r * TWSTEP);
+        }
+        Bfly<RAD, DIR>::run(&va[b * RAD]);
+        Bfly<RAD, DIR>::run(&vb[b * RAD]);
+    }
+}
+
+template <int N, int E, int LH, int RAD, int NS, int SW = 0>
+__device__ __forceinline__ void stage_store_pair(float4 *dst, const float2 *va, const float2 *vb, int lp, int t) {
+    constexpr int T = N / E, NB = E / RAD;
+#pragma unroll
+    for (int b = 0; b < NB; ++b) {
+        const int j = t + T * b;
+        const int base = (j / NS) * NS * RAD + j % NS;
+#pragma unroll
+        for (int r = 0; r < RAD; ++r)
+            dst[slot<SW>(base + r * NS) * LH + lp] =
+                make_float4(va[b * RAD + r].x, va[b * RAD + r].y, vb[b * RAD + r].x, vb[b * RAD + r].y);
+    }
+}
+
+// RegChain for line pairs (same stage order and barriers)
+template <int N, int E, int DIR, int LH, int S, int NS, int SW = 0> struct RegChainPair {
+    __device__ __forceinline__ static void run(float4 *work, float2 *va, float2 *vb, SmemTw<float2> tw, int lp, int t) {
+        if constexpr (S < Plan<N>::NST) {
+            constexpr int RP = Plan<N>::R[S - 1];
+            constexpr int RAD = Plan<N>::R[S];
+            __syncthreads();
+            stage_store_pair<N, E, LH, RP, NS / RP, SW>(work, va, vb, lp, t);
+            __syncthreads();
+            stage_load_pair<N, E, LH, RAD, SW>(work, va, vb, lp, t);
+            stage_compute_pair<N, E, DIR, RAD, NS>(va, vb, tw, t);
+            RegChainPair<N, E, DIR, LH, S + 1, NS * RAD, SW>::run(work, va, vb, tw, lp, t);
+        }
+    }
+};
+
 // Second transform straight from the registers of a first one (requires the
 // plan's first and last radix to be equal).
 template <typename C, int N, int E, int DIR, int L, int LP, int SW = 0, typename TW>

@@ -118,6 +118,21 @@ template <typename R_, typename K_, int N> struct Box {
             zt1grid = sms * (b1 > 0 ? b1 : 1);
             zt5grid = sms * (b5 > 0 ? b5 : 1);
             zt9grid = sms * (b9 > 0 ? b9 : 1);
+            if constexpr (kPair) {
+                CUDA_TRY(prep(k_kick_fft_z_pair<N, ZST1P, ZB1P>, ZSM1P));
+                CUDA_TRY(prep(k_density_r2c_z_pair<N, ZST5P, ZB5P>, ZSM5P));
+                CUDA_TRY(prep(k_c2r_z_pair<N, ZST9P, ZB9P>, ZSM9P));
+                int b1p = 0, b5p = 0, b9p = 0;
+                CUDA_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&b1p, k_kick_fft_z_pair<N, ZST1P, ZB1P>,
+                                                                       Z::NT / 2, ZSM1P));
+                CUDA_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&b5p, k_density_r2c_z_pair<N, ZST5P, ZB5P>,
+                                                                       Z::NT / 2, ZSM5P));
+                CUDA_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&b9p, k_c2r_z_pair<N, ZST9P, ZB9P>,
+                                                                       Z::NT / 2, ZSM9P));
+                zt1pgrid = sms * (b1p > 0 ? b1p : 1);
+                zt5pgrid = sms * (b5p > 0 ? b5p : 1);
+                zt9pgrid = sms * (b9p > 0 ? b9p : 1);
+            }
         }
         if constexpr (kTma) {
             CUDA_TRY(prep(k_yx_tma<R, K, N, 1, 0, -1>, TT::SMEM));
@@ -130,6 +145,19 @@ template <typename R_, typename K_, int N> struct Box {
             CUDA_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&bx, k_yx_tma<R, K, N, 2, 1, 0>, TX::NT, TX::SMEM));
             ygrid = sms * (by > 0 ? by : 1);
             xgrid = sms * (bx > 0 ? bx : 1);
+            if constexpr (kPair) {
+                CUDA_TRY(prep(k_yx_tma_pair<N, 1, 0, -1, PSTY, PBY>, TPY::SMEM));
+                CUDA_TRY(prep(k_yx_tma_pair<N, 1, 0, +1, PSTY, PBY>, TPY::SMEM));
+                CUDA_TRY(prep(k_yx_tma_pair<N, 2, 1, 0, PSTX, PBX>, TPX::SMEM));
+                CUDA_TRY(prep(k_yx_tma_pair<N, 2, 2, 0, PSTX, PBX>, TPX::SMEM));
+                int py = 0, px = 0;
+                CUDA_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&py, k_yx_tma_pair<N, 1, 0, -1, PSTY, PBY>,
+                                                                       TPY::NT, TPY::SMEM));
+                CUDA_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&px, k_yx_tma_pair<N, 2, 1, 0, PSTX, PBX>,
+                                                                       TPX::NT, TPX::SMEM));
+                pygrid = sms * (py > 0 ? py : 1);
+                pxgrid = sms * (px > 0 ? px : 1);
+            }
         }
         done_on.insert(dev);
         return "";
@@ -150,8 +178,25 @@ template <typename R_, typename K_, int N> struct Box {
     static constexpr size_t ZSM5 = kZT ? ZST5 * ZT<(kZT ? N : 256)>::SLOT5 + 64 + tw_bytes<C>(N) : 0;
     static constexpr size_t ZSM9 = kZT ? ZST9 * ZT<(kZT ? N : 256)>::SLOT9 + 64 + tw_bytes<C>(N) : 0;
     static inline int zt1grid = 0, zt5grid = 0, zt9grid = 0;  // persistent grids of the bulk-copy z passes
+    // the paired z passes (two rows per thread, 256 threads; kPair below):
+    // ring slots, resident blocks per SM, shared memory and persistent grids
+    static constexpr int ZST1P = 2, ZB1P = 2, ZST5P = 2, ZB5P = 3, ZST9P = 3, ZB9P = 2;
+    static constexpr size_t ZSM1P = kZT ? ZST1P * ZT<(kZT ? N : 256)>::SLOT1 + 64 + tw_bytes<C>(N) : 0;
+    static constexpr size_t ZSM5P = kZT ? ZST5P * ZT<(kZT ? N : 256)>::SLOT5 + 64 + tw_bytes<C>(N) : 0;
+    static constexpr size_t ZSM9P = kZT ? ZST9P * ZT<(kZT ? N : 256)>::SLOT9 + 64 + tw_bytes<C>(N) : 0;
+    static inline int zt1pgrid = 0, zt5pgrid = 0, zt9pgrid = 0;
     using TT = TmaTile<R, K, N, 1>;
     using TX = TmaTile<R, K, N, 2>;
+    // FP32 passes at N = 512 with two lines per thread: the y/x passes
+    // (k_yx_tma_pair, the same tiles and maps as TT/TX; ring slots and resident
+    // blocks per SM of the y and x passes below) and the z passes
+    // (k_*_z_pair, ZST*P/ZB*P above).  IFDM_NO_PAIR selects the one-line kernels.
+    static constexpr bool kPair = N == 512 && std::is_same<R, float>::value && std::is_same<K, float>::value;
+    static constexpr int PSTY = 2, PBY = 3, PSTX = 2, PBX = 3;
+    using TPY = TmaPair<512, PSTY, PBY>;
+    using TPX = TmaPair<512, PSTX, PBX>;
+    static_assert(!kPair || (TT::L == TPY::L && TX::L == TPX::L), "pair kernels share the tensor maps");
+    static inline int pygrid = 0, pxgrid = 0;
     static inline int zgrid = 0;             // persistent grid of the pipelined P5
     static inline int ygrid = 0, xgrid = 0;  // persistent grids of the TMA y and x passes
 
@@ -173,6 +218,18 @@ template <typename R_, typename K_, int N> struct Box {
             if (tm && (p == 1 || p == 5 || p == 9)) {
                 using Z = ZT<N>;
                 const int nz = int(size_t(N) * N / Z::L);
+                if constexpr (kPair) {
+                    if (std::getenv("IFDM_NO_PAIR") == nullptr) {
+                        const unsigned q = Z::NT / 2;
+                        if (p == 1)
+                            k_kick_fft_z_pair<N, ZST1P, ZB1P><<<zt1pgrid, q, ZSM1P, s>>>(psi, phi, ts, tw, nz);
+                        else if (p == 5)
+                            k_density_r2c_z_pair<N, ZST5P, ZB5P><<<zt5pgrid, q, ZSM5P, s>>>(psi, rhok, ts, tw, nz);
+                        else
+                            k_c2r_z_pair<N, ZST9P, ZB9P><<<zt9pgrid, q, ZSM9P, s>>>(rhok, phi, ts, wr, wt, tw, nz / 2);
+                        return;
+                    }
+                }
                 if (p == 1)
                     k_kick_fft_z_tma<N, ZST1, ZB1><<<zt1grid, Z::NT, ZSM1, s>>>(psi, phi, ts, tw, nz);
                 else if (p == 5)
@@ -197,6 +254,21 @@ template <typename R_, typename K_, int N> struct Box {
                 const int tcx = int(size_t(N) * N / TX::L), thx = int(size_t(N) * NHP / TX::L);
                 const unsigned gy = unsigned(ygrid), gx = unsigned(xgrid), ny = TT::NT, nx = TX::NT;
                 const size_t sy = TT::SMEM, sx = TX::SMEM;
+                if constexpr (kPair) {
+                    if (std::getenv("IFDM_NO_PAIR") == nullptr) {
+                        const unsigned py = unsigned(pygrid), px = unsigned(pxgrid), qy = TPY::NT, qx = TPX::NT;
+                        const size_t my = TPY::SMEM, mx = TPX::SMEM;
+                        switch (p) {
+                            case 2: k_yx_tma_pair<N, 1, 0, -1, PSTY, PBY><<<py, qy, my, s>>>(tm[0], psi, N, N, tcy, ts, drift, tw); break;
+                            case 3: k_yx_tma_pair<N, 2, 1, 0, PSTX, PBX><<<px, qx, mx, s>>>(tm[1], psi, N, N, tcx, ts, drift, tw); break;
+                            case 4: k_yx_tma_pair<N, 1, 0, +1, PSTY, PBY><<<py, qy, my, s>>>(tm[0], psi, N, N, tcy, ts, drift, tw); break;
+                            case 6: k_yx_tma_pair<N, 1, 0, -1, PSTY, PBY><<<py, qy, my, s>>>(tm[2], rhok, NHP, NH, thy, ts, drift, tw); break;
+                            case 7: k_yx_tma_pair<N, 2, 2, 0, PSTX, PBX><<<px, qx, mx, s>>>(tm[3], rhok, NHP, NH, thx, ts, drift, tw); break;
+                            case 8: k_yx_tma_pair<N, 1, 0, +1, PSTY, PBY><<<py, qy, my, s>>>(tm[2], rhok, NHP, NH, thy, ts, drift, tw); break;
+                        }
+                        return;
+                    }
+                }
                 switch (p) {
                     case 2: k_yx_tma<R, K, N, 1, 0, -1><<<gy, ny, sy, s>>>(tm[0], psi, N, N, tcy, ts, 2, drift, tw); break;
                     case 3: k_yx_tma<R, K, N, 2, 1, 0><<<gx, nx, sx, s>>>(tm[1], psi, N, N, tcx, ts, 3, drift, tw); break;

@@ -190,4 +190,137 @@ __global__ void __launch_bounds__(TmaTile<R, K, N, AXIS>::NT, TmaTile<R, K, N, A
     }
 }
 
+// FP32 y/x passes with two lines per thread (fft_engine.cuh, *_pair): the
+// same 8-line tiles, tensor maps, modes and arithmetic as k_yx_tma<float,
+// float, N>, with 256 threads per tile and 128-bit exchanges, twiddle loads
+// shared by two lines and 16-byte global stores.  ST ring slots, MINB
+// resident blocks per SM.
+template <int N, int ST, int MINB> struct TmaPair {
+    static constexpr int L = 8, LH = L / 2;
+    static constexpr int E = Plan<N>::E, T = N / E, NT = LH * T;
+    static constexpr int BOXR = N < 256 ? N : 256;
+    static constexpr size_t TILE_BYTES = size_t(N) * L * sizeof(float2);
+    static constexpr size_t TWOFF = ST * TILE_BYTES + 64;
+    static constexpr size_t SMEM = TWOFF + tw_bytes<float2>(N);
+    static_assert(Plan<N>::R[0] == Plan<N>::R[Plan<N>::NST - 1], "chained transforms need equal first/last radix");
+    static_assert(SMEM <= 227 * 1024, "shared memory per block");
+};
+
+template <int N, int AXIS, int MODE, int DIR, int ST, int MINB>
+__global__ void __launch_bounds__(TmaPair<N, ST, MINB>::NT, MINB)
+    k_yx_tma_pair(const __grid_constant__ CUtensorMap map, float2 *__restrict__ data, int W, int VW, int ntiles,
+                  TState *__restrict__ ts, const float2 *__restrict__ drift, const float2 *__restrict__ tw) {
+    using TP = TmaPair<N, ST, MINB>;
+    constexpr int L = TP::L, LH = TP::LH, T = TP::T, E = TP::E;
+    constexpr int R0 = Plan<N>::R[0];
+    constexpr int SW = 1;  // the slot swizzle of the 8-line FP32 exchange tile (fft_engine.cuh)
+    extern __shared__ __align__(128) unsigned char smraw[];
+    float2 *bufs = reinterpret_cast<float2 *>(smraw);
+    uint64_t *bar = reinterpret_cast<uint64_t *>(smraw + ST * TP::TILE_BYTES);
+    const int tid = threadIdx.x;
+    const int lp = tid % LH, t = tid / LH;
+    int *err = ts ? &ts->err : nullptr;
+    if (tid == 0) {
+        for (int s = 0; s < ST; ++s) mbar_init(&bar[s], 1);
+        mbar_init_fence();
+        prefetch_tmap(&map);
+    }
+    float2 *stw = reinterpret_cast<float2 *>(smraw + TP::TWOFF);
+    stage_twiddles(stw, tw, N);
+    const SmemTw<float2> tws{stw};
+    __syncthreads();
+    const int my_n = blockIdx.x < (unsigned)ntiles ? (ntiles - 1 - (int)blockIdx.x) / (int)gridDim.x + 1 : 0;
+    auto issue = [&](int i) {
+        const long tile = (long)blockIdx.x + (long)i * gridDim.x;
+        const int s = i % ST;
+        float2 *dst = bufs + (size_t)s * N * L;
+        const long g0 = tile * L;
+        mbar_arrive_expect_tx(&bar[s], (uint32_t)TP::TILE_BYTES);
+#pragma unroll
+        for (int h = 0; h < N; h += TP::BOXR) {
+            if (AXIS == 1) tma_load_3d(dst + (size_t)h * L, &map, 2 * int(g0 % W), h, int(g0 / W), &bar[s]);
+            else tma_load_2d(dst + (size_t)h * L, &map, 2 * int(g0), h, &bar[s]);
+        }
+    };
+    if (tid == 0)
+        for (int i = 0; i < ST - 1 && i < my_n; ++i) issue(i);
+    const size_t S = AXIS == 1 ? size_t(W) : size_t(N) * W;
+    for (int i = 0; i < my_n; ++i) {
+        const int s = i % ST;
+        if (tid == 0 && i + ST - 1 < my_n) issue(i + ST - 1);
+        const bool ok = mbar_wait(&bar[s], (uint32_t)((i / ST) & 1), err, 2);
+        if (!__syncthreads_and(ok)) {
+            // a load never completed: wait (bounded) for the copies still in flight, then leave
+            if (tid == 0)
+                for (int j = i; j < my_n && j <= i + ST - 1; ++j)
+                    mbar_wait(&bar[j % ST], (uint32_t)((j / ST) & 1), err, 2);
+            __syncthreads();
+            return;
+        }
+        // line g holds va, line g + 1 vb: W and L are even, so both lie in one row
+        const long g = ((long)blockIdx.x + (long)i * gridDim.x) * L + 2 * lp;
+        float2 va[E], vb[E];
+        float4 *wk = reinterpret_cast<float4 *>(bufs + (size_t)s * N * L);
+        stage_load_pair<N, E, LH, R0>(wk, va, vb, lp, t);
+        stage_compute_pair<N, E, (MODE == 0 ? DIR : -1), R0, 1>(va, vb, tws, t);
+        RegChainPair<N, E, (MODE == 0 ? DIR : -1), LH, 1, R0, SW>::run(wk, va, vb, tws, lp, t);
+        if (MODE != 0) {
+            // va[b*R0 + r] holds element n = (t + T*b) + r*N/R0 of the forward transform
+            if (MODE == 1) {
+                if (g == 0 && tid == 0) {
+                    const double inv = 1.0 / ((double)N * N * N);
+                    ts->cnext_re = ts->cre + (double)va[0].x * inv;
+                    ts->cnext_im = ts->cim + (double)va[0].y * inv;
+                }
+                const int y = int(g / N), z = int(g % N);
+                constexpr KSplit<float> inv3(1.0 / ((double)N * N * N));
+                const float2 da = cmul(__ldg(drift + y), __ldg(drift + z));
+                const float2 db = cmul(__ldg(drift + y), __ldg(drift + z + 1));
+                const float2 lfa = mkc(mulk(da.x, inv3.hi, inv3.lo), mulk(da.y, inv3.hi, inv3.lo));
+                const float2 lfb = mkc(mulk(db.x, inv3.hi, inv3.lo), mulk(db.y, inv3.hi, inv3.lo));
+#pragma unroll
+                for (int b = 0; b < E / R0; ++b)
+#pragma unroll
+                    for (int r = 0; r < R0; ++r) {
+                        const int n = t + T * b + r * (N / R0);
+                        const float2 dn = __ldg(drift + n);
+                        va[b * R0 + r] = cmul(va[b * R0 + r], cmul(lfa, dn));
+                        vb[b * R0 + r] = cmul(vb[b * R0 + r], cmul(lfb, dn));
+                    }
+            } else {
+                const int y = int(g / W), kz = int(g % W);
+                const int ky = kappa(y, N), ka = kappa(kz, N), kb = kappa(kz + 1, N);
+                const int k2a = ky * ky + ka * ka, k2b = ky * ky + kb * kb;
+#pragma unroll
+                for (int b = 0; b < E / R0; ++b)
+#pragma unroll
+                    for (int r = 0; r < R0; ++r) {
+                        const int kx = kappa(t + T * b + r * (N / R0), N);
+                        const int ea = kx * kx + k2a, eb = kx * kx + k2b;
+                        va[b * R0 + r] = cscale(va[b * R0 + r], ea == 0 ? 0.0f : -1.0f / float(ea));
+                        vb[b * R0 + r] = cscale(vb[b * R0 + r], eb == 0 ? 0.0f : -1.0f / float(eb));
+                    }
+            }
+            stage_compute_pair<N, E, +1, R0, 1>(va, vb, tws, t);
+            RegChainPair<N, E, +1, LH, 1, R0, SW>::run(wk, va, vb, tws, lp, t);
+        }
+        const int ca = int(g % W);
+        if (ca < VW) {
+            const size_t b0 = AXIS == 1 ? size_t(g / W) * N * W + size_t(ca) : size_t(g);
+            const bool both = ca + 1 < VW;
+#pragma unroll
+            for (int b = 0; b < E / R0; ++b)
+#pragma unroll
+                for (int r = 0; r < R0; ++r) {
+                    const size_t gi = b0 + size_t(t + T * b + r * (N / R0)) * S;
+                    const float2 a = va[b * R0 + r], c = vb[b * R0 + r];
+                    if (both) *reinterpret_cast<float4 *>(data + gi) = make_float4(a.x, a.y, c.x, c.y);
+                    else data[gi] = a;
+                }
+        }
+        fence_proxy_async_smem();
+        __syncthreads();
+    }
+}
+
 }  // namespace ifdm

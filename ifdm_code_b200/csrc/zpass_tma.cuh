@@ -148,6 +148,75 @@ __global__ void __launch_bounds__(ZT<N>::NT, MINB)
     }
 }
 
+// P1 with 256 threads per 8-row tile, two rows per thread (the kick of both
+// rows, then the paired transform: fft_engine.cuh, *_pair).  Same slots,
+// arithmetic and outputs as k_kick_fft_z_tma.
+template <int N, int ST, int MINB>
+__global__ void __launch_bounds__(ZT<N>::NT / 2, MINB)
+    k_kick_fft_z_pair(float2 *__restrict__ psi, const float *__restrict__ phi, TState *__restrict__ ts,
+                      const float2 *__restrict__ tw, int ntiles) {
+    using Z = ZT<N>;
+    using C = float2;
+    constexpr int L = Z::L, LH = L / 2, T = Z::T, E = Z::E, R0 = Z::R0, RL = Z::RL;
+    static_assert(Z::NT / 2 == LH * T, "one thread per row pair");
+    extern __shared__ __align__(128) unsigned char smraw[];
+    uint64_t *bar = reinterpret_cast<uint64_t *>(smraw + ST * Z::SLOT1);
+    const int tid = threadIdx.x, lp = tid % LH, t = tid / LH;
+    C *stw = reinterpret_cast<C *>(smraw + ST * Z::SLOT1 + 64);
+    stage_twiddles(stw, tw, N);
+    const SmemTw<C> tws{stw};
+    ring_init<ST>(bar);
+    const int my_n = ztiles_of_block(ntiles);
+    auto issue = [&](int i) {
+        const size_t row0 = size_t(blockIdx.x + (long)i * gridDim.x) * L;
+        unsigned char *slot = smraw + size_t(i % ST) * Z::SLOT1;
+        uint64_t *b = &bar[i % ST];
+        mbar_arrive_expect_tx(b, (uint32_t)(L * N * (sizeof(float2) + sizeof(float))));
+#pragma unroll 1
+        for (int r = 0; r < L; ++r) {
+            bulk_load(slot + size_t(r) * Z::PP * sizeof(float2), psi + (row0 + r) * N, N * sizeof(float2), b);
+            bulk_load(slot + Z::PSI_B + size_t(r) * Z::PF * sizeof(float), phi + (row0 + r) * N, N * sizeof(float),
+                      b);
+        }
+    };
+    if (tid == 0)
+        for (int i = 0; i < ST - 1 && i < my_n; ++i) issue(i);
+    const double cp = ts->coefP, cq = ts->coefQ, alpha = ts->alpha;
+    const C c0 = mkc((float)ts->cre, (float)ts->cim);
+    for (int i = 0; i < my_n; ++i) {
+        if (tid == 0 && i + ST - 1 < my_n) issue(i + ST - 1);
+        if (!ring_wait<ST>(bar, i, my_n, &ts->err)) return;
+        unsigned char *slot = smraw + size_t(i % ST) * Z::SLOT1;
+        const C *pa = reinterpret_cast<const C *>(slot) + (2 * lp) * Z::PP, *pb = pa + Z::PP;
+        const float *fa = reinterpret_cast<const float *>(slot + Z::PSI_B) + (2 * lp) * Z::PF, *fb = fa + Z::PF;
+        C va[E], vb[E];
+#pragma unroll
+        for (int b = 0; b < E / R0; ++b)
+#pragma unroll
+            for (int r = 0; r < R0; ++r) {
+                const int n = t + T * b + r * (N / R0);
+                const C ga = pa[n], gb = pb[n];
+                const double qa = cp * (double)fa[n] + cq * (double)cnorm2(ga) + alpha;
+                const double qb = cp * (double)fb[n] + cq * (double)cnorm2(gb) + alpha;
+                va[b * R0 + r] = cmul(ga, expmi<float>(qa)) - c0;
+                vb[b * R0 + r] = cmul(gb, expmi<float>(qb)) - c0;
+            }
+        stage_compute_pair<N, E, -1, R0, 1>(va, vb, tws, t);
+        RegChainPair<N, E, -1, LH, 1, R0, 1>::run(reinterpret_cast<float4 *>(slot), va, vb, tws, lp, t);
+        C *oa = psi + (size_t(blockIdx.x + (long)i * gridDim.x) * L + 2 * lp) * N, *ob = oa + N;
+#pragma unroll
+        for (int b = 0; b < E / RL; ++b)
+#pragma unroll
+            for (int r = 0; r < RL; ++r) {
+                const int n = t + T * b + r * (N / RL);
+                oa[n] = va[b * RL + r];
+                ob[n] = vb[b * RL + r];
+            }
+        fence_proxy_async_smem();
+        __syncthreads();
+    }
+}
+
 // ------------------------------------------------------------------- P5 ---
 template <int N, int ST, int MINB>
 __global__ void __launch_bounds__(ZT<N>::NT, MINB)
@@ -257,6 +326,127 @@ __global__ void __launch_bounds__(ZT<N>::NT, MINB)
     if ((tid & 31) == 0 && my_n > 0) atomic_max_nonneg(&ts->maxrho_bits, mx);
 }
 
+// P5 with 256 threads per 8-row tile: the inverse transform of psi runs two
+// rows per thread (fft_engine.cuh, *_pair: 128-bit exchanges, one twiddle
+// load per two rows), the packed density transform of the tile's 4 complex
+// lines one line per thread, so every thread works in both transforms (the
+// 512-thread kernel above idles half of its threads in the second one).
+// Same slots, arithmetic and outputs as k_density_r2c_z_tma.
+template <int N, int ST, int MINB>
+__global__ void __launch_bounds__(ZT<N>::NT / 2, MINB)
+    k_density_r2c_z_pair(float2 *__restrict__ psi, float2 *__restrict__ rhok, TState *__restrict__ ts,
+                         const float2 *__restrict__ tw, int ntiles) {
+    using Z = ZT<N>;
+    using C = float2;
+    constexpr int L = Z::L, T = Z::T, E = Z::E, R0 = Z::R0, RL = Z::RL, NT = Z::NT / 2;
+    constexpr int M = N / 2, NHP = Z::NHP;
+    constexpr int LH = L / 2;  // row pairs of the psi transform = packed lines of the density transform
+    static_assert(NT == LH * T, "one thread per row pair and per packed line");
+    extern __shared__ __align__(128) unsigned char smraw[];
+    uint64_t *bar = reinterpret_cast<uint64_t *>(smraw + ST * Z::SLOT5);
+    const int tid = threadIdx.x, lp = tid % LH, t = tid / LH;
+    C *stw = reinterpret_cast<C *>(smraw + ST * Z::SLOT5 + 64);
+    stage_twiddles(stw, tw, N);
+    const SmemTw<C> tws{stw};
+    ring_init<ST>(bar);
+    const int my_n = ztiles_of_block(ntiles);
+    auto issue = [&](int i) {
+        const size_t row0 = size_t(blockIdx.x + (long)i * gridDim.x) * L;
+        unsigned char *slot = smraw + size_t(i % ST) * Z::SLOT5;
+        uint64_t *b = &bar[i % ST];
+        mbar_arrive_expect_tx(b, (uint32_t)(L * N * sizeof(float2)));
+#pragma unroll 1
+        for (int r = 0; r < L; ++r)
+            bulk_load(slot + size_t(r) * Z::PP * sizeof(float2), psi + (row0 + r) * N, N * sizeof(float2), b);
+    };
+    if (tid == 0)
+        for (int i = 0; i < ST - 1 && i < my_n; ++i) issue(i);
+    const double mu = ts->mu;
+    const C c0 = mkc((float)ts->cre, (float)ts->cim);
+    double mx = 0.0;
+    for (int i = 0; i < my_n; ++i) {
+        if (tid == 0 && i + ST - 1 < my_n) issue(i + ST - 1);
+        if (!ring_wait<ST>(bar, i, my_n, &ts->err)) return;
+        unsigned char *slot = smraw + size_t(i % ST) * Z::SLOT5;
+        C *wk = reinterpret_cast<C *>(slot);
+        const size_t row0 = size_t(blockIdx.x + (long)i * gridDim.x) * L;
+        // inverse FFT of rows 2lp (va) and 2lp + 1 (vb), stage 0 from the landed rows
+        C va[E], vb[E];
+        const C *la = reinterpret_cast<const C *>(slot) + (2 * lp) * Z::PP, *lb = la + Z::PP;
+#pragma unroll
+        for (int b = 0; b < E / R0; ++b)
+#pragma unroll
+            for (int r = 0; r < R0; ++r) {
+                const int n = t + T * b + r * (N / R0);
+                va[b * R0 + r] = la[n];
+                vb[b * R0 + r] = lb[n];
+            }
+        stage_compute_pair<N, E, +1, R0, 1>(va, vb, tws, t);
+        RegChainPair<N, E, +1, LH, 1, R0, 1>::run(reinterpret_cast<float4 *>(wk), va, vb, tws, lp, t);
+        // psi = IFFT + c; rho = |psi|^2 - mu into the float tile that pairs
+        // rows p and p + 4 of element n: rt[(n*LH + p)*2 + h] holds row p + h*LH
+        float ra[E], rb[E];
+        C *oa = psi + (row0 + 2 * lp) * N, *ob = oa + N;
+#pragma unroll
+        for (int b = 0; b < E / RL; ++b)
+#pragma unroll
+            for (int r = 0; r < RL; ++r) {
+                const int n = t + T * b + r * (N / RL);
+                const C ga = va[b * RL + r] + c0, gb = vb[b * RL + r] + c0;
+                oa[n] = ga;
+                ob[n] = gb;
+                const double na = (double)cnorm2(ga), nb = (double)cnorm2(gb);
+                mx = fmax(mx, fmax(na, nb));
+                ra[b * RL + r] = (float)(na - mu);
+                rb[b * RL + r] = (float)(nb - mu);
+            }
+        float *rt = reinterpret_cast<float *>(slot);
+        __syncthreads();  // every thread is done with the exchange tile
+        const int rowa = 2 * lp, rowb = rowa + 1;
+#pragma unroll
+        for (int b = 0; b < E / RL; ++b)
+#pragma unroll
+            for (int r = 0; r < RL; ++r) {
+                const int n = t + T * b + r * (N / RL);
+                rt[(n * LH + rowa % LH) * 2 + rowa / LH] = ra[b * RL + r];
+                rt[(n * LH + rowb % LH) * 2 + rowb / LH] = rb[b * RL + r];
+            }
+        __syncthreads();
+        // packed line p = tid % LH: rho_p + i rho_{p+4}, forward FFT, one line per thread
+        const int p = lp;
+        C v[E];
+        {
+            const C *rp = reinterpret_cast<const C *>(rt);
+#pragma unroll
+            for (int b = 0; b < E / R0; ++b)
+#pragma unroll
+                for (int r = 0; r < R0; ++r) v[b * R0 + r] = rp[(t + T * b + r * (N / R0)) * LH + p];
+            stage_compute<C, N, E, -1, R0, 1>(v, tws, t);
+        }
+        RegChain<C, N, E, -1, LH, LH, 1, R0, 3>::run(wk, v, tws, p, t, true);
+        // Z_k in an [k][p] tile, then the two half spectra of each line
+        __syncthreads();
+#pragma unroll
+        for (int b = 0; b < E / RL; ++b)
+#pragma unroll
+            for (int r = 0; r < RL; ++r) wk[(t + T * b + r * (N / RL)) * LH + p] = v[b * RL + r];
+        __syncthreads();
+        for (int q = tid; q < LH * (M + 1); q += NT) {
+            const int pp = q % LH, k = q / LH;
+            const C zk = wk[k * LH + pp];
+            const C zc = cconj(wk[((N - k) % N) * LH + pp]);
+            const C s = cscale(zk + zc, 0.5f);
+            const C d = cscale(zk - zc, 0.5f);
+            rhok[(row0 + pp) * NHP + k] = s;
+            rhok[(row0 + pp + LH) * NHP + k] = mkc(d.y, -d.x);
+        }
+        fence_proxy_async_smem();
+        __syncthreads();
+    }
+    mx = warp_max(mx);
+    if ((tid & 31) == 0 && my_n > 0) atomic_max_nonneg(&ts->maxrho_bits, mx);
+}
+
 // ------------------------------------------------------------------- P9 ---
 template <int N, int ST, int MINB>
 __global__ void __launch_bounds__(ZT<N>::NT, MINB)
@@ -325,6 +515,100 @@ __global__ void __launch_bounds__(ZT<N>::NT, MINB)
                 ob[n] = fb;
                 if (n < lima) mx = fmax(mx, (double)fabsf(fa));
                 if (n < limb) mx = fmax(mx, (double)fabsf(fb));
+            }
+        fence_proxy_async_smem();
+        __syncthreads();
+    }
+    const double m = warp_max(mx);
+    if ((tid & 31) == 0) atomic_max_nonneg(&ts->maxphi_bits, m);
+}
+
+// P9 with 256 threads per 16-row tile: packed lines 2lp and 2lp + 1 (rows
+// 2lp, 2lp + 8 and 2lp + 1, 2lp + 9) per thread, the paired inverse
+// transform (fft_engine.cuh, *_pair).  Same slots, arithmetic and outputs as
+// k_c2r_z_tma.
+template <int N, int ST, int MINB>
+__global__ void __launch_bounds__(ZT<N>::NT / 2, MINB)
+    k_c2r_z_pair(const float2 *__restrict__ rhok, float *__restrict__ phi, TState *__restrict__ ts, long win_rows,
+                 int win_tail, const float2 *__restrict__ tw, int ntiles) {
+    using Z = ZT<N>;
+    using C = float2;
+    constexpr int L = Z::L, LH = L / 2, T = Z::T, E = Z::E, R0 = Z::R0, RL = Z::RL;
+    constexpr int M = N / 2, NHP = Z::NHP, ROWS = 2 * L;
+    static_assert(Z::NT / 2 == LH * T, "one thread per line pair");
+    extern __shared__ __align__(128) unsigned char smraw[];
+    uint64_t *bar = reinterpret_cast<uint64_t *>(smraw + ST * Z::SLOT9);
+    const int tid = threadIdx.x, lp = tid % LH, t = tid / LH;
+    C *stw = reinterpret_cast<C *>(smraw + ST * Z::SLOT9 + 64);
+    stage_twiddles(stw, tw, N);
+    const SmemTw<C> tws{stw};
+    ring_init<ST>(bar);
+    const int my_n = ztiles_of_block(ntiles);
+    auto issue = [&](int i) {
+        const size_t row0 = size_t(blockIdx.x + (long)i * gridDim.x) * ROWS;
+        unsigned char *slot = smraw + size_t(i % ST) * Z::SLOT9;
+        uint64_t *b = &bar[i % ST];
+        mbar_arrive_expect_tx(b, (uint32_t)(ROWS * NHP * sizeof(float2)));
+#pragma unroll 1
+        for (int r = 0; r < ROWS; ++r)
+            bulk_load(slot + size_t(r) * Z::PH * sizeof(float2), rhok + (row0 + r) * NHP, NHP * sizeof(float2), b);
+    };
+    if (tid == 0)
+        for (int i = 0; i < ST - 1 && i < my_n; ++i) issue(i);
+    constexpr KSplit<float> inv(1.0 / ((double)N * N * N));
+    double mx = 0.0;  // the running max on the FP64 pipe, which this pass leaves idle
+    // line l of the tile: Z = X_l + i X_{l+8} on the full circle (X_{N-k} = conj X_k)
+    auto packed = [&](const C *xa, const C *xb, int n) {
+        const int m = n <= M ? n : N - n;
+        C a = xa[m], b = xb[m];
+        if (m == 0 || m == M) {  // c2r ignores these imaginary parts
+            a.y = 0.f;
+            b.y = 0.f;
+        }
+        return n <= M ? mkc(a.x - b.y, a.y + b.x) : mkc(a.x + b.y, b.x - a.y);
+    };
+    for (int i = 0; i < my_n; ++i) {
+        if (tid == 0 && i + ST - 1 < my_n) issue(i + ST - 1);
+        if (!ring_wait<ST>(bar, i, my_n, &ts->err)) return;
+        unsigned char *slot = smraw + size_t(i % ST) * Z::SLOT9;
+        const C *xa0 = reinterpret_cast<const C *>(slot) + (2 * lp) * Z::PH, *xb0 = xa0 + L * Z::PH;
+        const C *xa1 = xa0 + Z::PH, *xb1 = xb0 + Z::PH;
+        C va[E], vb[E];
+#pragma unroll
+        for (int bb = 0; bb < E / R0; ++bb)
+#pragma unroll
+            for (int r = 0; r < R0; ++r) {
+                const int n = t + T * bb + r * (N / R0);
+                va[bb * R0 + r] = packed(xa0, xb0, n);
+                vb[bb * R0 + r] = packed(xa1, xb1, n);
+            }
+        stage_compute_pair<N, E, +1, R0, 1>(va, vb, tws, t);
+        RegChainPair<N, E, +1, LH, 1, R0, 1>::run(reinterpret_cast<float4 *>(slot), va, vb, tws, lp, t);
+        // line 2lp writes rows ra, ra + 8; line 2lp + 1 rows ra + 1, ra + 9
+        const long ra = long(blockIdx.x + (long)i * gridDim.x) * ROWS + 2 * lp;
+        const long rows[4] = {ra, ra + L, ra + 1, ra + 1 + L};
+        int lim[4];
+#pragma unroll
+        for (int q = 0; q < 4; ++q)  // elements of rows below win_rows, and the first win_tail of row win_rows
+            lim[q] = rows[q] < win_rows ? N : (rows[q] == win_rows ? win_tail : 0);
+        float *o0 = phi + size_t(rows[0]) * N, *o1 = phi + size_t(rows[1]) * N;
+        float *o2 = phi + size_t(rows[2]) * N, *o3 = phi + size_t(rows[3]) * N;
+#pragma unroll
+        for (int bb = 0; bb < E / RL; ++bb)
+#pragma unroll
+            for (int r = 0; r < RL; ++r) {
+                const int n = t + T * bb + r * (N / RL);
+                const C za = va[bb * RL + r], zb = vb[bb * RL + r];
+                const float f0 = mulk(za.x, inv.hi, inv.lo), f1 = mulk(za.y, inv.hi, inv.lo);
+                const float f2 = mulk(zb.x, inv.hi, inv.lo), f3 = mulk(zb.y, inv.hi, inv.lo);
+                o0[n] = f0;
+                o1[n] = f1;
+                o2[n] = f2;
+                o3[n] = f3;
+                if (n < lim[0]) mx = fmax(mx, (double)fabsf(f0));
+                if (n < lim[1]) mx = fmax(mx, (double)fabsf(f1));
+                if (n < lim[2]) mx = fmax(mx, (double)fabsf(f2));
+                if (n < lim[3]) mx = fmax(mx, (double)fabsf(f3));
             }
         fence_proxy_async_smem();
         __syncthreads();

@@ -11,8 +11,10 @@ numpy on the benchmark's own inputs:
 * two fixed-mode leap-frog steps of the benchmark configuration (512^3,
   xmax 5, mfdm 2.5e-24 eV, self-interaction at 0.01 rad per step at the
   densest cell, the step scale that reaches a = 0.5 in 1000 steps) in every
-  precision mode, through the TMA passes and through the plain passes, against
-  the oracle's two steps from the same psi;
+  precision mode, through the TMA passes and through the plain passes (FP32
+  also through the one-line-per-thread TMA y/x kernels that IFDM_NO_PAIR
+  selects instead of the two-line ones), against the oracle's two steps from
+  the same psi;
 * phi of the initial Poisson solve against the oracle's.
 
 The oracle needs about 7 GB of host memory and ~7 s per step on 16 cores at
@@ -56,11 +58,15 @@ def case512():
     return dict(psi0=psi0, C=C, g=g, phi0=phi0, ref=ref, a=a_ref, A0=bench.A0, xmax=bench.XMAX, mfdm=bench.MFDM)
 
 
-def _run(case, prec, tma, monkeypatch):
+def _run(case, prec, tma, monkeypatch, pair=True):
     if tma:
         monkeypatch.delenv("IFDM_NO_TMA", raising=False)
     else:
         monkeypatch.setenv("IFDM_NO_TMA", "1")
+    if pair:
+        monkeypatch.delenv("IFDM_NO_PAIR", raising=False)
+    else:
+        monkeypatch.setenv("IFDM_NO_PAIR", "1")
     with Simulation(case["mfdm"], case["g"], case["xmax"], N, precision=prec) as s:
         s.set_psi(case["psi0"], case["A0"])
         phi = s.get_phi() if prec == "fp64" else None
@@ -90,6 +96,14 @@ def test_reduced_precision_512_matches_oracle(case512, prec, tma, monkeypatch):
     err = rel_l2(psi, case512["ref"])
     print(f"{prec} 512^3 {'tma' if tma else 'plain'}: psi rel L2 vs oracle {err:.3e}")
     assert err <= REDUCED_TOL[prec]
+
+
+def test_fp32_512_one_line_kernels_match_oracle(case512, monkeypatch):
+    psi, _, st = _run(case512, "fp32", True, monkeypatch, pair=False)
+    assert st["device_error"] == 0
+    err = rel_l2(psi, case512["ref"])
+    print(f"fp32 512^3 tma one-line y/x kernels: psi rel L2 vs oracle {err:.3e}")
+    assert err <= REDUCED_TOL["fp32"]
 
 
 def test_fft3d_512_matches_numpy():

@@ -308,15 +308,22 @@ __device__ __forceinline__ void stage_load(const SrcT *src, C *v, int l, int t) 
         }
 }
 
+// twiddle r of butterfly k in the stage (NS, RAD) from a flat table (the
+// per-stage tables of the paired kernels add an overload further down)
+template <int DIR, int N, int RAD, int NS, typename C, typename TW>
+__device__ __forceinline__ C tw_apply(C a, TW tw, int k, int r) {
+    return twmul<DIR, N>(a, tw, k * r * (N / (NS * RAD)));
+}
+
 template <typename C, int N, int E, int DIR, int RAD, int NS, typename TW>
 __device__ __forceinline__ void stage_compute(C *v, TW tw, int t) {
-    constexpr int T = N / E, NB = E / RAD, TWSTEP = N / (NS * RAD);
+    constexpr int T = N / E, NB = E / RAD;
 #pragma unroll
     for (int b = 0; b < NB; ++b) {
         const int k = (t + T * b) % NS;
         if (NS > 1) {
 #pragma unroll
-            for (int r = 1; r < RAD; ++r) v[b * RAD + r] = twmul<DIR, N>(v[b * RAD + r], tw, k * r * TWSTEP);
+            for (int r = 1; r < RAD; ++r) v[b * RAD + r] = tw_apply<DIR, N, RAD, NS>(v[b * RAD + r], tw, k, r);
         }
         Bfly<RAD, DIR>::run(&v[b * RAD]);
     }
@@ -373,14 +380,79 @@ __device__ __forceinline__ void fft_regs(const SrcT *src, C *work, C *v, TW tw, 
 // one 128-bit shared-memory access and each twiddle load serves both lines
 // (half the shared-memory instructions and twiddle wavefronts of one line per
 // thread).  va holds line 2lp, vb line 2lp + 1, in the RegChain order.
-template <int DIR> __device__ __forceinline__ void twmul_pair(float2 &a, float2 &b, SmemTw<float2> tw, int m) {
-    const float4 q = reinterpret_cast<const float4 *>(tw.p)[m];
-    const float hy = DIR < 0 ? q.y : -q.y, ry = DIR < 0 ? q.w : -q.w;
+//
+// StagedTw: the FP32 twiddles as per-stage tables in shared memory, which the
+// paired kernels use: the stage with NS = product of the earlier radices and
+// radix RAD keeps w^(k r N/(NS RAD)) at [(r-1) NS + k] (k < NS, r = 1 ..
+// RAD-1).  The threads of a warp hold consecutive k, so their loads hit
+// consecutive 16-byte entries, where the flat table's entries k r N/(NS RAD)
+// lie r N/(NS RAD) entries apart (for the radix-8 stages of 512 points 128 r
+// bytes: the same banks).  Same values as the flat table, so the same results.
+template <int N, class P = Plan<N>> struct StagedTw {
+    const float4 *p;
+    // first entry of the stage whose earlier radices multiply to ns
+    static constexpr int offset(int ns) {
+        int o = 0, q = 1;
+        for (int s = 0; s < P::NST; ++s) {
+            if (q == ns) return o;
+            if (q > 1) o += (P::R[s] - 1) * q;
+            q *= P::R[s];
+        }
+        return o;
+    }
+    static constexpr int entries() { return offset(N); }
+};
+template <int N, class P = Plan<N>> __host__ __device__ constexpr size_t staged_tw_bytes() {
+    return size_t(StagedTw<N, P>::entries()) * 16;
+}
+// Flat-table index of per-stage entry i (stages S.., Q = product of the
+// radices before S, O = first entry of stage S).
+template <int N, class P, int S = 0, int Q = 1, int O = 0>
+__device__ __forceinline__ int staged_src(int i) {
+    if constexpr (S >= P::NST) {
+        return 0;
+    } else {
+        constexpr int RAD = P::R[S];
+        constexpr int CNT = Q > 1 ? (RAD - 1) * Q : 0;
+        if (i >= O && i < O + CNT) {
+            const int j = i - O;
+            return (j % Q) * (j / Q + 1) * (N / (Q * RAD));
+        }
+        return staged_src<N, P, S + 1, Q * RAD, O + CNT>(i);
+    }
+}
+// Fill the per-stage tables from the flat FP32 table (hi, remainder pairs);
+// all threads of the block, the caller syncs.
+template <int N, class P = Plan<N>> __device__ __forceinline__ void stage_twiddles_staged(float4 *dst, const float2 *src) {
+    const float4 *s4 = reinterpret_cast<const float4 *>(src);
+    for (int i = threadIdx.x; i < StagedTw<N, P>::entries(); i += blockDim.x) dst[i] = __ldg(s4 + staged_src<N, P>(i));
+}
+
+__device__ __forceinline__ void twmul_pair_q(float2 &a, float2 &b, float4 q, int dir) {
+    const float hy = dir < 0 ? q.y : -q.y, ry = dir < 0 ? q.w : -q.w;
     float cr = fmaf(a.x, q.z, -a.y * ry), ci = fmaf(a.x, ry, a.y * q.z);
     a = make_float2(fmaf(a.x, q.x, fmaf(-a.y, hy, cr)), fmaf(a.x, hy, fmaf(a.y, q.x, ci)));
     cr = fmaf(b.x, q.z, -b.y * ry);
     ci = fmaf(b.x, ry, b.y * q.z);
     b = make_float2(fmaf(b.x, q.x, fmaf(-b.y, hy, cr)), fmaf(b.x, hy, fmaf(b.y, q.x, ci)));
+}
+// twiddle r of butterfly k in the stage (NS, RAD), from either table
+template <int DIR, int N, int RAD, int NS>
+__device__ __forceinline__ void twmul_pair(float2 &a, float2 &b, SmemTw<float2> tw, int k, int r) {
+    twmul_pair_q(a, b, reinterpret_cast<const float4 *>(tw.p)[k * r * (N / (NS * RAD))], DIR);
+}
+template <int DIR, int N, int RAD, int NS, class P>
+__device__ __forceinline__ void twmul_pair(float2 &a, float2 &b, StagedTw<N, P> tw, int k, int r) {
+    twmul_pair_q(a, b, tw.p[StagedTw<N, P>::offset(NS) + (r - 1) * NS + k], DIR);
+}
+// one line from the per-stage tables (the single-line stages of the paired kernels)
+template <int DIR, int N, int RAD, int NS, typename C, class P>
+__device__ __forceinline__ C tw_apply(C a, StagedTw<N, P> tw, int k, int r) {
+    static_assert(sizeof(C) == 8, "per-stage tables hold FP32 twiddles");
+    const float4 q = tw.p[StagedTw<N, P>::offset(NS) + (r - 1) * NS + k];
+    const float hy = DIR < 0 ? q.y : -q.y, ry = DIR < 0 ? q.w : -q.w;
+    const float cr = fmaf(a.x, q.z, -a.y * ry), ci = fmaf(a.x, ry, a.y * q.z);
+    return make_float2(fmaf(a.x, q.x, fmaf(-a.y, hy, cr)), fmaf(a.x, hy, fmaf(a.y, q.x, ci)));
 }
 
 template <int N, int E, int LH, int RAD, int SW = 0>
@@ -396,15 +468,15 @@ __device__ __forceinline__ void stage_load_pair(const float4 *src, float2 *va, f
         }
 }
 
-template <int N, int E, int DIR, int RAD, int NS>
-__device__ __forceinline__ void stage_compute_pair(float2 *va, float2 *vb, SmemTw<float2> tw, int t) {
-    constexpr int T = N / E, NB = E / RAD, TWSTEP = N / (NS * RAD);
+template <int N, int E, int DIR, int RAD, int NS, typename TW>
+__device__ __forceinline__ void stage_compute_pair(float2 *va, float2 *vb, TW tw, int t) {
+    constexpr int T = N / E, NB = E / RAD;
 #pragma unroll
     for (int b = 0; b < NB; ++b) {
         const int k = (t + T * b) % NS;
         if (NS > 1) {
 #pragma unroll
-            for (int r = 1; r < RAD; ++r) twmul_pair<DIR>(va[b * RAD + r], vb[b * RAD + r], tw, k * r * TWSTEP);
+            for (int r = 1; r < RAD; ++r) twmul_pair<DIR, N, RAD, NS>(va[b * RAD + r], vb[b * RAD + r], tw, k, r);
         }
         Bfly<RAD, DIR>::run(&va[b * RAD]);
         Bfly<RAD, DIR>::run(&vb[b * RAD]);
@@ -427,7 +499,8 @@ __device__ __forceinline__ void stage_store_pair(float4 *dst, const float2 *va, 
 
 // RegChain for line pairs (same stage order and barriers)
 template <int N, int E, int DIR, int LH, int S, int NS, int SW = 0> struct RegChainPair {
-    __device__ __forceinline__ static void run(float4 *work, float2 *va, float2 *vb, SmemTw<float2> tw, int lp, int t) {
+    template <typename TW>
+    __device__ __forceinline__ static void run(float4 *work, float2 *va, float2 *vb, TW tw, int lp, int t) {
         if constexpr (S < Plan<N>::NST) {
             constexpr int RP = Plan<N>::R[S - 1];
             constexpr int RAD = Plan<N>::R[S];

@@ -162,9 +162,9 @@ __global__ void __launch_bounds__(ZT<N>::NT / 2, MINB)
     extern __shared__ __align__(128) unsigned char smraw[];
     uint64_t *bar = reinterpret_cast<uint64_t *>(smraw + ST * Z::SLOT1);
     const int tid = threadIdx.x, lp = tid % LH, t = tid / LH;
-    C *stw = reinterpret_cast<C *>(smraw + ST * Z::SLOT1 + 64);
-    stage_twiddles(stw, tw, N);
-    const SmemTw<C> tws{stw};
+    float4 *stw = reinterpret_cast<float4 *>(smraw + ST * Z::SLOT1 + 64);
+    stage_twiddles_staged<N>(stw, tw);
+    const StagedTw<N> tws{stw};
     ring_init<ST>(bar);
     const int my_n = ztiles_of_block(ntiles);
     auto issue = [&](int i) {
@@ -345,9 +345,9 @@ __global__ void __launch_bounds__(ZT<N>::NT / 2, MINB)
     extern __shared__ __align__(128) unsigned char smraw[];
     uint64_t *bar = reinterpret_cast<uint64_t *>(smraw + ST * Z::SLOT5);
     const int tid = threadIdx.x, lp = tid % LH, t = tid / LH;
-    C *stw = reinterpret_cast<C *>(smraw + ST * Z::SLOT5 + 64);
-    stage_twiddles(stw, tw, N);
-    const SmemTw<C> tws{stw};
+    float4 *stw = reinterpret_cast<float4 *>(smraw + ST * Z::SLOT5 + 64);
+    stage_twiddles_staged<N>(stw, tw);
+    const StagedTw<N> tws{stw};
     ring_init<ST>(bar);
     const int my_n = ztiles_of_block(ntiles);
     auto issue = [&](int i) {
@@ -539,9 +539,9 @@ __global__ void __launch_bounds__(ZT<N>::NT / 2, MINB)
     extern __shared__ __align__(128) unsigned char smraw[];
     uint64_t *bar = reinterpret_cast<uint64_t *>(smraw + ST * Z::SLOT9);
     const int tid = threadIdx.x, lp = tid % LH, t = tid / LH;
-    C *stw = reinterpret_cast<C *>(smraw + ST * Z::SLOT9 + 64);
-    stage_twiddles(stw, tw, N);
-    const SmemTw<C> tws{stw};
+    float4 *stw = reinterpret_cast<float4 *>(smraw + ST * Z::SLOT9 + 64);
+    stage_twiddles_staged<N>(stw, tw);
+    const StagedTw<N> tws{stw};
     ring_init<ST>(bar);
     const int my_n = ztiles_of_block(ntiles);
     auto issue = [&](int i) {

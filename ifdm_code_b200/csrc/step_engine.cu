@@ -107,14 +107,14 @@ template <typename R_, typename K_, int N> struct Box {
             zgrid = sms * (b5 > 0 ? b5 : 1);
         }
         if constexpr (kZT) {
-            using Z = ZT<N>;
-            CUDA_TRY(prep(k_kick_fft_z_tma<N, ZST1, ZB1>, ZSM1));
-            CUDA_TRY(prep(k_density_r2c_z_tma<N, ZST5, ZB5>, ZSM5));
-            CUDA_TRY(prep(k_c2r_z_tma<N, ZST9, ZB9>, ZSM9));
+            using Z = ZT<N, R>;
+            CUDA_TRY(prep(k_kick_fft_z_tma<N, ZST1, ZB1, R>, ZSM1));
+            CUDA_TRY(prep(k_density_r2c_z_tma<N, ZST5, ZB5, R>, ZSM5));
+            CUDA_TRY(prep(k_c2r_z_tma<N, ZST9, ZB9, R>, ZSM9));
             int b1 = 0, b5 = 0, b9 = 0;
-            CUDA_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&b1, k_kick_fft_z_tma<N, ZST1, ZB1>, Z::NT, ZSM1));
-            CUDA_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&b5, k_density_r2c_z_tma<N, ZST5, ZB5>, Z::NT, ZSM5));
-            CUDA_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&b9, k_c2r_z_tma<N, ZST9, ZB9>, Z::NT, ZSM9));
+            CUDA_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&b1, k_kick_fft_z_tma<N, ZST1, ZB1, R>, Z::NT, ZSM1));
+            CUDA_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&b5, k_density_r2c_z_tma<N, ZST5, ZB5, R>, Z::NT, ZSM5));
+            CUDA_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&b9, k_c2r_z_tma<N, ZST9, ZB9, R>, Z::NT, ZSM9));
             zt1grid = sms * (b1 > 0 ? b1 : 1);
             zt5grid = sms * (b5 > 0 ? b5 : 1);
             zt9grid = sms * (b9 > 0 ? b9 : 1);
@@ -169,21 +169,23 @@ template <typename R_, typename K_, int N> struct Box {
     // than three plain blocks), and pipelined P1/P9 gained nothing.
     static constexpr bool kTma = N >= 128;
     static constexpr bool kZPipe = N >= 128 && N <= 512 && std::is_same<R, float>::value && std::is_same<K, float>::value;
-    // FP32 z passes fed by bulk copies (zpass_tma.cuh) for N >= 256; ring
-    // depth and resident blocks per SM of P1, P5 and P9
-    static constexpr bool kZT = N >= 256 && std::is_same<R, float>::value && std::is_same<K, float>::value;
+    // z passes fed by bulk copies (zpass_tma.cuh): FP32 for N >= 256, FP64
+    // at 256 and 512 (8 FP32 or 4 FP64 rows per tile); ring depth and
+    // resident blocks per SM of P1, P5 and P9
+    static constexpr bool kZT = N >= 256 && std::is_same<R, K>::value && (std::is_same<R, float>::value || N <= 512);
     static constexpr int ZST1 = 2, ZST5 = 3, ZST9 = 3, ZB1 = N >= 1024 ? 1 : 2, ZB5 = ZB1, ZB9 = ZB1;
+    using ZG = ZT<(kZT ? N : 256), R>;
     // ring slots, the mbarriers (64 bytes) and the staged twiddle table
-    static constexpr size_t ZSM1 = kZT ? ZST1 * ZT<(kZT ? N : 256)>::SLOT1 + 64 + tw_bytes<C>(N) : 0;
-    static constexpr size_t ZSM5 = kZT ? ZST5 * ZT<(kZT ? N : 256)>::SLOT5 + 64 + tw_bytes<C>(N) : 0;
-    static constexpr size_t ZSM9 = kZT ? ZST9 * ZT<(kZT ? N : 256)>::SLOT9 + 64 + tw_bytes<C>(N) : 0;
+    static constexpr size_t ZSM1 = kZT ? ZST1 * ZG::SLOT1 + 64 + tw_bytes<C>(N) : 0;
+    static constexpr size_t ZSM5 = kZT ? ZST5 * ZG::SLOT5 + 64 + tw_bytes<C>(N) : 0;
+    static constexpr size_t ZSM9 = kZT ? ZST9 * ZG::SLOT9 + 64 + tw_bytes<C>(N) : 0;
     static inline int zt1grid = 0, zt5grid = 0, zt9grid = 0;  // persistent grids of the bulk-copy z passes
     // the paired z passes (two rows per thread, 256 threads; kPair below):
     // ring slots, resident blocks per SM, shared memory and persistent grids
     static constexpr int ZST1P = 2, ZB1P = 2, ZST5P = 2, ZB5P = 3, ZST9P = 3, ZB9P = 2;
-    static constexpr size_t ZSM1P = kZT ? ZST1P * ZT<(kZT ? N : 256)>::SLOT1 + 64 + tw_bytes<C>(N) : 0;
-    static constexpr size_t ZSM5P = kZT ? ZST5P * ZT<(kZT ? N : 256)>::SLOT5 + 64 + tw_bytes<C>(N) : 0;
-    static constexpr size_t ZSM9P = kZT ? ZST9P * ZT<(kZT ? N : 256)>::SLOT9 + 64 + tw_bytes<C>(N) : 0;
+    static constexpr size_t ZSM1P = kZT ? ZST1P * ZG::SLOT1 + 64 + tw_bytes<C>(N) : 0;
+    static constexpr size_t ZSM5P = kZT ? ZST5P * ZG::SLOT5 + 64 + tw_bytes<C>(N) : 0;
+    static constexpr size_t ZSM9P = kZT ? ZST9P * ZG::SLOT9 + 64 + tw_bytes<C>(N) : 0;
     static inline int zt1pgrid = 0, zt5pgrid = 0, zt9pgrid = 0;
     using TT = TmaTile<R, K, N, 1>;
     using TX = TmaTile<R, K, N, 2>;
@@ -216,7 +218,7 @@ template <typename R_, typename K_, int N> struct Box {
         const unsigned nt = TL::NT;
         if constexpr (kZT) {
             if (tm && (p == 1 || p == 5 || p == 9)) {
-                using Z = ZT<N>;
+                using Z = ZT<N, R>;
                 const int nz = int(size_t(N) * N / Z::L);
                 if constexpr (kPair) {
                     if (std::getenv("IFDM_NO_PAIR") == nullptr) {
@@ -231,11 +233,11 @@ template <typename R_, typename K_, int N> struct Box {
                     }
                 }
                 if (p == 1)
-                    k_kick_fft_z_tma<N, ZST1, ZB1><<<zt1grid, Z::NT, ZSM1, s>>>(psi, phi, ts, tw, nz);
+                    k_kick_fft_z_tma<N, ZST1, ZB1, R><<<zt1grid, Z::NT, ZSM1, s>>>(psi, phi, ts, tw, nz);
                 else if (p == 5)
-                    k_density_r2c_z_tma<N, ZST5, ZB5><<<zt5grid, Z::NT, ZSM5, s>>>(psi, rhok, ts, tw, nz);
+                    k_density_r2c_z_tma<N, ZST5, ZB5, R><<<zt5grid, Z::NT, ZSM5, s>>>(psi, rhok, ts, tw, nz);
                 else
-                    k_c2r_z_tma<N, ZST9, ZB9><<<zt9grid, Z::NT, ZSM9, s>>>(rhok, phi, ts, wr, wt, tw, nz / 2);
+                    k_c2r_z_tma<N, ZST9, ZB9, R><<<zt9grid, Z::NT, ZSM9, s>>>(rhok, phi, ts, wr, wt, tw, nz / 2);
                 return;
             }
         }

@@ -1,4 +1,4 @@
-// zpass_tma.cuh -- persistent z passes fed by bulk copies (FP32, N >= 256).
+// zpass_tma.cuh -- persistent z passes fed by bulk copies (FP32 N >= 256, FP64 256 and 512).
 //
 // The z passes work on whole rows (z fastest), which are contiguous in HBM.
 // Each CTA keeps a ring of ST slots; thread 0 keeps ST-1 tiles of rows in
@@ -37,31 +37,35 @@
 
 namespace ifdm {
 
-// Tile geometry of the FP32 z passes: 8 complex lines per tile (NT threads).
-template <int N> struct ZT {
-    static constexpr int L = 8;
+// Tile geometry of the z passes: L complex rows per tile (NT threads), 64
+// bytes of the [n][l] exchange tile per element index: 8 FP32 rows or 4 FP64
+// rows.  Landed rows are padded by 2 elements (16 bytes FP32, 32 bytes FP64),
+// which puts the rows of a tile in different banks for the row-fastest first
+// stage.
+template <int N, typename R = float> struct ZT {
+    using C = cx<R>;
+    static constexpr int L = sizeof(R) == 4 ? 8 : 4;
     static constexpr int E = Plan<N>::E;
     static constexpr int T = N / E;
     static constexpr int NT = L * T;
     static constexpr int R0 = Plan<N>::R[0];
     static constexpr int RL = Plan<N>::R[Plan<N>::NST - 1];
-    static constexpr int PP = N + 2;  // float2 per landed psi row (16-byte pad)
-    static constexpr int PF = N + 4;  // floats per landed phi row (16-byte pad)
-    static constexpr int NHP = half_pitch<float>(N);
-    static constexpr int PH = NHP + 2;  // float2 per landed half row (16-byte pad)
-    static constexpr size_t XCH = size_t(N) * L * sizeof(float2);  // [n][l] exchange tile
-    // P1 slot: 8 psi rows, then 8 phi rows
-    static constexpr size_t PSI_B = size_t(L) * PP * sizeof(float2);
-    static constexpr size_t SLOT1 = (PSI_B + size_t(L) * PF * sizeof(float) + 127) / 128 * 128;
-    // P5 slot: 8 psi rows
+    static constexpr int PP = N + 2;  // complex elements per landed psi row
+    static constexpr int PF = N + 4;  // reals per landed phi row
+    static constexpr int NHP = half_pitch<R>(N);
+    static constexpr int PH = NHP + 2;  // complex elements per landed half row
+    static constexpr size_t XCH = size_t(N) * L * sizeof(C);  // [n][l] exchange tile
+    // P1 slot: L psi rows, then L phi rows
+    static constexpr size_t PSI_B = size_t(L) * PP * sizeof(C);
+    static constexpr size_t SLOT1 = (PSI_B + size_t(L) * PF * sizeof(R) + 127) / 128 * 128;
+    // P5 slot: L psi rows
     static constexpr size_t SLOT5 = (PSI_B + 127) / 128 * 128;
-    // P9 slot: 16 half rows
-    static constexpr size_t SLOT9 = (size_t(2 * L) * PH * sizeof(float2) + 127) / 128 * 128;
+    // P9 slot: 2L half rows
+    static constexpr size_t SLOT9 = (size_t(2 * L) * PH * sizeof(C) + 127) / 128 * 128;
     static_assert(XCH <= PSI_B && XCH <= SLOT9, "the exchange tile fits the landed rows");
     static_assert(E % R0 == 0 && E % RL == 0 && R0 == RL, "register chain: equal first and last radix");
-    static_assert((N * sizeof(float2)) % 16 == 0 && (NHP * sizeof(float2)) % 16 == 0 &&
-                      (PP * sizeof(float2)) % 16 == 0 && (PF * sizeof(float)) % 16 == 0 &&
-                      (PH * sizeof(float2)) % 16 == 0,
+    static_assert((N * sizeof(C)) % 16 == 0 && (NHP * sizeof(C)) % 16 == 0 && (PP * sizeof(C)) % 16 == 0 &&
+                      (PF * sizeof(R)) % 16 == 0 && (PH * sizeof(C)) % 16 == 0,
                   "bulk copies need 16-byte sizes and destinations");
 };
 
@@ -89,12 +93,12 @@ __device__ __forceinline__ int ztiles_of_block(int ntiles) {
 }
 
 // ------------------------------------------------------------------- P1 ---
-template <int N, int ST, int MINB>
-__global__ void __launch_bounds__(ZT<N>::NT, MINB)
-    k_kick_fft_z_tma(float2 *__restrict__ psi, const float *__restrict__ phi, TState *__restrict__ ts,
-                     const float2 *__restrict__ tw, int ntiles) {
-    using Z = ZT<N>;
-    using C = float2;
+template <int N, int ST, int MINB, typename R = float>
+__global__ void __launch_bounds__(ZT<N, R>::NT, MINB)
+    k_kick_fft_z_tma(cx<R> *__restrict__ psi, const R *__restrict__ phi, TState *__restrict__ ts,
+                     const cx<R> *__restrict__ tw, int ntiles) {
+    using Z = ZT<N, R>;
+    using C = cx<R>;
     constexpr int L = Z::L, T = Z::T, E = Z::E, R0 = Z::R0, RL = Z::RL;
     extern __shared__ __align__(128) unsigned char smraw[];
     uint64_t *bar = reinterpret_cast<uint64_t *>(smraw + ST * Z::SLOT1);
@@ -108,24 +112,24 @@ __global__ void __launch_bounds__(ZT<N>::NT, MINB)
         const size_t row0 = size_t(blockIdx.x + (long)i * gridDim.x) * L;
         unsigned char *slot = smraw + size_t(i % ST) * Z::SLOT1;
         uint64_t *b = &bar[i % ST];
-        mbar_arrive_expect_tx(b, (uint32_t)(L * N * (sizeof(float2) + sizeof(float))));
+        mbar_arrive_expect_tx(b, (uint32_t)(L * N * (sizeof(C) + sizeof(R))));
 #pragma unroll 1
         for (int r = 0; r < L; ++r) {
-            bulk_load(slot + size_t(r) * Z::PP * sizeof(float2), psi + (row0 + r) * N, N * sizeof(float2), b);
-            bulk_load(slot + Z::PSI_B + size_t(r) * Z::PF * sizeof(float), phi + (row0 + r) * N, N * sizeof(float),
+            bulk_load(slot + size_t(r) * Z::PP * sizeof(C), psi + (row0 + r) * N, N * sizeof(C), b);
+            bulk_load(slot + Z::PSI_B + size_t(r) * Z::PF * sizeof(R), phi + (row0 + r) * N, N * sizeof(R),
                       b);
         }
     };
     if (tid == 0)
         for (int i = 0; i < ST - 1 && i < my_n; ++i) issue(i);
     const double cp = ts->coefP, cq = ts->coefQ, alpha = ts->alpha;
-    const C c0 = mkc((float)ts->cre, (float)ts->cim);
+    const C c0 = mkc((R)ts->cre, (R)ts->cim);
     for (int i = 0; i < my_n; ++i) {
         if (tid == 0 && i + ST - 1 < my_n) issue(i + ST - 1);
         if (!ring_wait<ST>(bar, i, my_n, &ts->err)) return;
         unsigned char *slot = smraw + size_t(i % ST) * Z::SLOT1;
         const C *lp = reinterpret_cast<const C *>(slot) + l * Z::PP;
-        const float *lf = reinterpret_cast<const float *>(slot + Z::PSI_B) + l * Z::PF;
+        const R *lf = reinterpret_cast<const R *>(slot + Z::PSI_B) + l * Z::PF;
         C v[E];
 #pragma unroll
         for (int b = 0; b < E / R0; ++b)
@@ -134,7 +138,7 @@ __global__ void __launch_bounds__(ZT<N>::NT, MINB)
                 const int n = t + T * b + r * (N / R0);
                 const C g = lp[n];
                 const double p = cp * (double)lf[n] + cq * (double)cnorm2(g) + alpha;
-                v[b * R0 + r] = cmul(g, expmi<float>(p)) - c0;
+                v[b * R0 + r] = cmul(g, expmi<R>(p)) - c0;
             }
         stage_compute<C, N, E, -1, R0, 1>(v, tws, t);
         RegChain<C, N, E, -1, L, L, 1, R0, 1>::run(reinterpret_cast<C *>(slot), v, tws, l, t, true);
@@ -218,12 +222,12 @@ __global__ void __launch_bounds__(ZT<N>::NT / 2, MINB)
 }
 
 // ------------------------------------------------------------------- P5 ---
-template <int N, int ST, int MINB>
-__global__ void __launch_bounds__(ZT<N>::NT, MINB)
-    k_density_r2c_z_tma(float2 *__restrict__ psi, float2 *__restrict__ rhok, TState *__restrict__ ts,
-                        const float2 *__restrict__ tw, int ntiles) {
-    using Z = ZT<N>;
-    using C = float2;
+template <int N, int ST, int MINB, typename R = float>
+__global__ void __launch_bounds__(ZT<N, R>::NT, MINB)
+    k_density_r2c_z_tma(cx<R> *__restrict__ psi, cx<R> *__restrict__ rhok, TState *__restrict__ ts,
+                        const cx<R> *__restrict__ tw, int ntiles) {
+    using Z = ZT<N, R>;
+    using C = cx<R>;
     constexpr int L = Z::L, T = Z::T, E = Z::E, R0 = Z::R0, RL = Z::RL, NT = Z::NT;
     constexpr int M = N / 2, NHP = Z::NHP;
     constexpr int LH = L / 2;  // packed complex lines of the density transform
@@ -242,15 +246,15 @@ __global__ void __launch_bounds__(ZT<N>::NT, MINB)
         const size_t row0 = size_t(blockIdx.x + (long)i * gridDim.x) * L;
         unsigned char *slot = smraw + size_t(i % ST) * Z::SLOT5;
         uint64_t *b = &bar[i % ST];
-        mbar_arrive_expect_tx(b, (uint32_t)(L * N * sizeof(float2)));
+        mbar_arrive_expect_tx(b, (uint32_t)(L * N * sizeof(C)));
 #pragma unroll 1
         for (int r = 0; r < L; ++r)
-            bulk_load(slot + size_t(r) * Z::PP * sizeof(float2), psi + (row0 + r) * N, N * sizeof(float2), b);
+            bulk_load(slot + size_t(r) * Z::PP * sizeof(C), psi + (row0 + r) * N, N * sizeof(C), b);
     };
     if (tid == 0)
         for (int i = 0; i < ST - 1 && i < my_n; ++i) issue(i);
     const double mu = ts->mu;
-    const C c0 = mkc((float)ts->cre, (float)ts->cim);
+    const C c0 = mkc((R)ts->cre, (R)ts->cim);
     double mx = 0.0;
     for (int i = 0; i < my_n; ++i) {
         if (tid == 0 && i + ST - 1 < my_n) issue(i + ST - 1);
@@ -267,11 +271,11 @@ __global__ void __launch_bounds__(ZT<N>::NT, MINB)
             for (int r = 0; r < R0; ++r) v[b * R0 + r] = lp[t + T * b + r * (N / R0)];
         stage_compute<C, N, E, +1, R0, 1>(v, tws, t);
         RegChain<C, N, E, +1, L, L, 1, R0, 1>::run(wk, v, tws, l, t, true);
-        // psi = IFFT + c; rho = |psi|^2 - mu into a float tile that pairs rows
-        // p and p+4 of element n: rt[(n*LH + p)*2 + h] holds row p + h*LH
-        // (conflict-free stores of the [l, t] layout and float2 loads of the
+        // psi = IFFT + c; rho = |psi|^2 - mu into a real tile that pairs rows
+        // p and p+LH of element n: rt[(n*LH + p)*2 + h] holds row p + h*LH
+        // (conflict-free stores of the [l, t] layout and complex loads of the
         // packed layout)
-        float rho[E];
+        R rho[E];
         C *out = psi + (row0 + l) * N;
 #pragma unroll
         for (int b = 0; b < E / RL; ++b)
@@ -281,9 +285,9 @@ __global__ void __launch_bounds__(ZT<N>::NT, MINB)
                 out[t + T * b + r * (N / RL)] = g;
                 const double n2 = (double)cnorm2(g);
                 mx = fmax(mx, n2);
-                rho[b * RL + r] = (float)(n2 - mu);
+                rho[b * RL + r] = (R)(n2 - mu);
             }
-        float *rt = reinterpret_cast<float *>(slot);
+        R *rt = reinterpret_cast<R *>(slot);
         __syncthreads();  // every thread is done with the exchange tile
 #pragma unroll
         for (int b = 0; b < E / RL; ++b)
@@ -314,8 +318,8 @@ __global__ void __launch_bounds__(ZT<N>::NT, MINB)
             const int pp = q % LH, k = q / LH;
             const C zk = wk[k * LH + pp];
             const C zc = cconj(wk[((N - k) % N) * LH + pp]);
-            const C s = cscale(zk + zc, 0.5f);
-            const C d = cscale(zk - zc, 0.5f);
+            const C s = cscale(zk + zc, R(0.5));
+            const C d = cscale(zk - zc, R(0.5));
             rhok[(row0 + pp) * NHP + k] = s;
             rhok[(row0 + pp + LH) * NHP + k] = mkc(d.y, -d.x);
         }
@@ -448,12 +452,12 @@ __global__ void __launch_bounds__(ZT<N>::NT / 2, MINB)
 }
 
 // ------------------------------------------------------------------- P9 ---
-template <int N, int ST, int MINB>
-__global__ void __launch_bounds__(ZT<N>::NT, MINB)
-    k_c2r_z_tma(const float2 *__restrict__ rhok, float *__restrict__ phi, TState *__restrict__ ts, long win_rows,
-                int win_tail, const float2 *__restrict__ tw, int ntiles) {
-    using Z = ZT<N>;
-    using C = float2;
+template <int N, int ST, int MINB, typename R = float>
+__global__ void __launch_bounds__(ZT<N, R>::NT, MINB)
+    k_c2r_z_tma(const cx<R> *__restrict__ rhok, R *__restrict__ phi, TState *__restrict__ ts, long win_rows,
+                int win_tail, const cx<R> *__restrict__ tw, int ntiles) {
+    using Z = ZT<N, R>;
+    using C = cx<R>;
     constexpr int L = Z::L, T = Z::T, E = Z::E, R0 = Z::R0, RL = Z::RL;
     constexpr int M = N / 2, NHP = Z::NHP, ROWS = 2 * L;
     extern __shared__ __align__(128) unsigned char smraw[];
@@ -468,14 +472,14 @@ __global__ void __launch_bounds__(ZT<N>::NT, MINB)
         const size_t row0 = size_t(blockIdx.x + (long)i * gridDim.x) * ROWS;
         unsigned char *slot = smraw + size_t(i % ST) * Z::SLOT9;
         uint64_t *b = &bar[i % ST];
-        mbar_arrive_expect_tx(b, (uint32_t)(ROWS * NHP * sizeof(float2)));
+        mbar_arrive_expect_tx(b, (uint32_t)(ROWS * NHP * sizeof(C)));
 #pragma unroll 1
         for (int r = 0; r < ROWS; ++r)
-            bulk_load(slot + size_t(r) * Z::PH * sizeof(float2), rhok + (row0 + r) * NHP, NHP * sizeof(float2), b);
+            bulk_load(slot + size_t(r) * Z::PH * sizeof(C), rhok + (row0 + r) * NHP, NHP * sizeof(C), b);
     };
     if (tid == 0)
         for (int i = 0; i < ST - 1 && i < my_n; ++i) issue(i);
-    constexpr KSplit<float> inv(1.0 / ((double)N * N * N));
+    constexpr KSplit<R> inv(1.0 / ((double)N * N * N));
     double mx = 0.0;  // the running max on the FP64 pipe, which this pass leaves idle
     for (int i = 0; i < my_n; ++i) {
         if (tid == 0 && i + ST - 1 < my_n) issue(i + ST - 1);
@@ -492,8 +496,8 @@ __global__ void __launch_bounds__(ZT<N>::NT, MINB)
                 const int m = n <= M ? n : N - n;
                 C a = xa[m], b = xb[m];
                 if (m == 0 || m == M) {  // c2r ignores these imaginary parts
-                    a.y = 0.f;
-                    b.y = 0.f;
+                    a.y = R(0);
+                    b.y = R(0);
                 }
                 v[bb * R0 + r] = n <= M ? mkc(a.x - b.y, a.y + b.x) : mkc(a.x + b.y, b.x - a.y);
             }
@@ -503,18 +507,18 @@ __global__ void __launch_bounds__(ZT<N>::NT, MINB)
         // elements of rows below win_rows, and the first win_tail of row win_rows, are in the window
         const int lima = ra < win_rows ? N : (ra == win_rows ? win_tail : 0);
         const int limb = rb < win_rows ? N : (rb == win_rows ? win_tail : 0);
-        float *oa = phi + size_t(ra) * N, *ob = phi + size_t(rb) * N;
+        R *oa = phi + size_t(ra) * N, *ob = phi + size_t(rb) * N;
 #pragma unroll
         for (int bb = 0; bb < E / RL; ++bb)
 #pragma unroll
             for (int r = 0; r < RL; ++r) {
                 const int n = t + T * bb + r * (N / RL);
                 const C z = v[bb * RL + r];
-                const float fa = mulk(z.x, inv.hi, inv.lo), fb = mulk(z.y, inv.hi, inv.lo);
+                const R fa = mulk(z.x, inv.hi, inv.lo), fb = mulk(z.y, inv.hi, inv.lo);
                 oa[n] = fa;
                 ob[n] = fb;
-                if (n < lima) mx = fmax(mx, (double)fabsf(fa));
-                if (n < limb) mx = fmax(mx, (double)fabsf(fb));
+                if (n < lima) mx = fmax(mx, fabs((double)fa));
+                if (n < limb) mx = fmax(mx, fabs((double)fb));
             }
         fence_proxy_async_smem();
         __syncthreads();

@@ -240,6 +240,35 @@ def test_tma_passes_match_plain_passes(ic128, tmp_path, prec, monkeypatch):
     assert rel_l2(out[True], out[False]) <= (1e-13 if prec == "fp64" else 2e-6)
 
 
+@pytest.mark.parametrize("prec", ["fp64", "fp32"])
+def test_bulk_copy_z_passes_match_plain_passes_256(prec, monkeypatch):
+    """At 256^3 the z passes run the bulk-copy kernels (FP64 with 4-row tiles,
+    FP32 with 8-row tiles) and the y/x passes the TMA kernels; three fixed
+    steps against the plain kernels from the same psi."""
+    import bench
+    from ifdm_code_b200.synthetic_ic import zeldovich_psi
+
+    N = 256
+    psi0 = zeldovich_psi(N, xmax=bench.XMAX, seed=0, a=bench.A0, mfdm=bench.MFDM)
+    C = bench.dt_scale_for(N)
+    g = bench.g_for_phase(N, psi0, C, 0.1)
+    out = {}
+    for tma in (True, False):
+        if tma:
+            monkeypatch.delenv("IFDM_NO_TMA", raising=False)
+        else:
+            monkeypatch.setenv("IFDM_NO_TMA", "1")
+        with Simulation(bench.MFDM, g, bench.XMAX, N, precision=prec) as s:
+            s.set_psi(psi0, bench.A0)
+            s.step(3, C)
+            out[tma] = (s.get_psi(), s.get_phi(), s.state())
+    assert out[True][2]["device_error"] == 0
+    assert out[True][2]["a"] == out[False][2]["a"]
+    tol = 1e-13 if prec == "fp64" else 2e-6
+    assert rel_l2(out[True][0], out[False][0]) <= tol
+    assert rel_l2(out[True][1], out[False][1]) <= tol
+
+
 def test_strong_self_interaction_follows_oracle(tmp_path):
     """The self-interaction strength the 512^3 precision configuration names
     (0.1 rad per step at the densest cell) with its step scale (0.696 of the

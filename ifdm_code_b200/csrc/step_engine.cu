@@ -182,9 +182,11 @@ template <typename R_, typename K_, int N> struct Box {
     static inline int zt1grid = 0, zt5grid = 0, zt9grid = 0;  // persistent grids of the bulk-copy z passes
     // the paired z passes (two rows per thread, 256 threads; kPair below):
     // ring slots, resident blocks per SM, shared memory and persistent grids
-    // (P1 with one slot at three blocks per SM measured 0.641 -> 0.593 ms
-    // against two slots at two blocks: the blocks overlap each other's loads)
-    static constexpr int ZST1P = 1, ZB1P = 3, ZST5P = 2, ZB5P = 3, ZST9P = 3, ZB9P = 2;
+    // (P1 and P9 with one slot at three blocks per SM measured 0.641 -> 0.593
+    // ms and 0.273 -> 0.244 ms against two or three slots at two blocks: the
+    // blocks overlap each other's loads; the y passes at one slot and four
+    // blocks measured slower, 0.392 -> 0.43 ms)
+    static constexpr int ZST1P = 1, ZB1P = 3, ZST5P = 2, ZB5P = 3, ZST9P = 1, ZB9P = 3;
     static constexpr size_t ZSM1P = kZT ? ZST1P * ZG::SLOT1 + 64 + tw_bytes<C>(N) : 0;
     static constexpr size_t ZSM5P = kZT ? ZST5P * ZG::SLOT5 + 64 + tw_bytes<C>(N) : 0;
     static constexpr size_t ZSM9P = kZT ? ZST9P * ZG::SLOT9 + 64 + tw_bytes<C>(N) : 0;

@@ -334,8 +334,11 @@ __global__ void __launch_bounds__(ZT<N, R>::NT, MINB)
 // rows per thread (fft_engine.cuh, *_pair: 128-bit exchanges, one twiddle
 // load per two rows), the packed density transform of the tile's 4 complex
 // lines one line per thread, so every thread works in both transforms (the
-// 512-thread kernel above idles half of its threads in the second one).
-// Same slots, arithmetic and outputs as k_density_r2c_z_tma.
+// 512-thread kernel above idles half of its threads in the second one).  The
+// packed line of thread lp is rho_{2lp} + i rho_{2lp+1}, its own two rows,
+// so the density goes from registers straight into the second transform.
+// Same slots and outputs as k_density_r2c_z_tma, the same arithmetic but
+// for which rows share a packed line.
 template <int N, int ST, int MINB>
 __global__ void __launch_bounds__(ZT<N>::NT / 2, MINB)
     k_density_r2c_z_pair(float2 *__restrict__ psi, float2 *__restrict__ rhok, TState *__restrict__ ts,
@@ -387,9 +390,12 @@ __global__ void __launch_bounds__(ZT<N>::NT / 2, MINB)
             }
         stage_compute_pair<N, E, +1, R0, 1>(va, vb, tws, t);
         RegChainPair<N, E, +1, LH, 1, R0, 1>::run(reinterpret_cast<float4 *>(wk), va, vb, tws, lp, t);
-        // psi = IFFT + c; rho = |psi|^2 - mu into the float tile that pairs
-        // rows p and p + 4 of element n: rt[(n*LH + p)*2 + h] holds row p + h*LH
-        float ra[E], rb[E];
+        // psi = IFFT + c; rho = |psi|^2 - mu; the thread's two rows 2lp and
+        // 2lp + 1 form the packed line rho_{2lp} + i rho_{2lp+1}, whose
+        // elements are already the first-stage inputs of the next transform
+        // (first radix = last radix): no exchange through shared memory
+        const int p = lp;
+        C v[E];
         C *oa = psi + (row0 + 2 * lp) * N, *ob = oa + N;
 #pragma unroll
         for (int b = 0; b < E / RL; ++b)
@@ -401,32 +407,10 @@ __global__ void __launch_bounds__(ZT<N>::NT / 2, MINB)
                 ob[n] = gb;
                 const double na = (double)cnorm2(ga), nb = (double)cnorm2(gb);
                 mx = fmax(mx, fmax(na, nb));
-                ra[b * RL + r] = (float)(na - mu);
-                rb[b * RL + r] = (float)(nb - mu);
+                v[b * RL + r] = mkc((float)(na - mu), (float)(nb - mu));
             }
-        float *rt = reinterpret_cast<float *>(slot);
-        __syncthreads();  // every thread is done with the exchange tile
-        const int rowa = 2 * lp, rowb = rowa + 1;
-#pragma unroll
-        for (int b = 0; b < E / RL; ++b)
-#pragma unroll
-            for (int r = 0; r < RL; ++r) {
-                const int n = t + T * b + r * (N / RL);
-                rt[(n * LH + rowa % LH) * 2 + rowa / LH] = ra[b * RL + r];
-                rt[(n * LH + rowb % LH) * 2 + rowb / LH] = rb[b * RL + r];
-            }
-        __syncthreads();
-        // packed line p = tid % LH: rho_p + i rho_{p+4}, forward FFT, one line per thread
-        const int p = lp;
-        C v[E];
-        {
-            const C *rp = reinterpret_cast<const C *>(rt);
-#pragma unroll
-            for (int b = 0; b < E / R0; ++b)
-#pragma unroll
-                for (int r = 0; r < R0; ++r) v[b * R0 + r] = rp[(t + T * b + r * (N / R0)) * LH + p];
-            stage_compute<C, N, E, -1, R0, 1>(v, tws, t);
-        }
+        // forward FFT of the packed line, one line per thread
+        stage_compute<C, N, E, -1, R0, 1>(v, tws, t);
         RegChain<C, N, E, -1, LH, LH, 1, R0, 3>::run(wk, v, tws, p, t, true);
         // Z_k in an [k][p] tile, then the two half spectra of each line
         __syncthreads();
@@ -441,8 +425,8 @@ __global__ void __launch_bounds__(ZT<N>::NT / 2, MINB)
             const C zc = cconj(wk[((N - k) % N) * LH + pp]);
             const C s = cscale(zk + zc, 0.5f);
             const C d = cscale(zk - zc, 0.5f);
-            rhok[(row0 + pp) * NHP + k] = s;
-            rhok[(row0 + pp + LH) * NHP + k] = mkc(d.y, -d.x);
+            rhok[(row0 + 2 * pp) * NHP + k] = s;
+            rhok[(row0 + 2 * pp + 1) * NHP + k] = mkc(d.y, -d.x);
         }
         fence_proxy_async_smem();
         __syncthreads();

@@ -405,6 +405,13 @@ template <int N, class P = Plan<N>> struct StagedTw {
 template <int N, class P = Plan<N>> __host__ __device__ constexpr size_t staged_tw_bytes() {
     return size_t(StagedTw<N, P>::entries()) * 16;
 }
+// 512 = 8 * 8 * 8: stage NS = 8 at [0, 56), NS = 64 at [56, 504)
+static_assert(StagedTw<512>::offset(8) == 0 && StagedTw<512>::offset(64) == 56 && StagedTw<512>::entries() == 504,
+              "per-stage table layout");
+// 1024 = 4 * 8 * 8 * 4: NS = 4, 32, 256 at 0, 28, 252; 1020 entries
+static_assert(StagedTw<1024>::offset(4) == 0 && StagedTw<1024>::offset(32) == 28 &&
+                  StagedTw<1024>::offset(256) == 252 && StagedTw<1024>::entries() == 1020,
+              "per-stage table layout");
 // Flat-table index of per-stage entry i (stages S.., Q = product of the
 // radices before S, O = first entry of stage S).
 template <int N, class P, int S = 0, int Q = 1, int O = 0>

@@ -1,7 +1,7 @@
 // timestep.cuh -- Timestep_criteria (src/CosmoBEC_MPI.cpp:19-78) on the device.
 //
 // One block.  Thread 0 turns the max reductions of the previous passes into
-// the three step criteria, advances the scale factor and integrates
+// the three step criteria and advances the scale factor; three warps integrate
 //   dt_KE = int da/(H a^3), dt_PE = int da/(H a^2), dt_QI = int da/(H a^4)
 // (integrands src/struct3D.h:127-146) with the QUADPACK method the reference
 // gets from GSL's qags: one 21-point Gauss-Kronrod rule, accepted when its
@@ -80,11 +80,69 @@ static __device__ void qk21(int n, double H0, double Om, double a, double b, dou
     *resasc = sasc;
 }
 
+// The same rule evaluated by a whole warp: lanes 0-9 take the left nodes,
+// 10-19 the right ones, 20 the centre (the integrand's two pow calls are the
+// cost), then every lane sums the 21 values in qk21's order, so the results
+// are bit-identical to qk21 and equal on all lanes.  Called by all 32 lanes.
+static __device__ void qk21_warp(int n, double H0, double Om, double a, double b, double *res, double *abserr,
+                                 double *resasc) {
+    const int lane = threadIdx.x & 31;
+    const double c = 0.5 * (a + b), h = 0.5 * (b - a);
+    double x = c;
+    if (lane < 20) {
+        const double dxj = h * c_gk_x[lane % 10];
+        x = lane < 10 ? c - dxj : c + dxj;
+    }
+    const double f = lane <= 20 ? qk_integrand(n, x, H0, Om) : 0.0;
+    const double fc = __shfl_sync(0xffffffffu, f, 20);
+    double kron = fc * c_gk_wk[10], gauss = 0.0, sabs = fabs(kron);
+    double fl[10], fr[10];
+#pragma unroll
+    for (int j = 0; j < 10; ++j) {
+        fl[j] = __shfl_sync(0xffffffffu, f, j);
+        fr[j] = __shfl_sync(0xffffffffu, f, 10 + j);
+    }
+    for (int j = 1; j < 10; j += 2) {
+        const double s = fl[j] + fr[j];
+        gauss += c_gk_wg[j / 2] * s;
+        kron += c_gk_wk[j] * s;
+        sabs += c_gk_wk[j] * (fabs(fl[j]) + fabs(fr[j]));
+    }
+    for (int j = 0; j < 10; j += 2) {
+        const double s = fl[j] + fr[j];
+        kron += c_gk_wk[j] * s;
+        sabs += c_gk_wk[j] * (fabs(fl[j]) + fabs(fr[j]));
+    }
+    const double mean = 0.5 * kron;
+    double sasc = c_gk_wk[10] * fabs(fc - mean);
+    for (int j = 0; j < 10; ++j) sasc += c_gk_wk[j] * (fabs(fl[j] - mean) + fabs(fr[j] - mean));
+    double err = fabs((kron - gauss) * h);
+    kron *= h;
+    sabs *= fabs(h);
+    sasc *= fabs(h);
+    if (sasc != 0.0 && err != 0.0) {
+        const double scale = pow(200.0 * err / sasc, 1.5);
+        err = (scale < 1.0) ? sasc * scale : sasc;
+    }
+    const double eps = 2.220446049250313e-16, dmin = 2.2250738585072014e-308;
+    if (sabs > dmin / (50.0 * eps)) err = fmax(err, 50.0 * eps * sabs);
+    *res = kron;
+    *abserr = err;
+    *resasc = sasc;
+}
+
 #define IFDM_QLIMIT 64
-// Returns 0 on success, 1 when the interval limit was reached.
+// Returns 0 on success, 1 when the interval limit was reached.  WARP: the
+// rule is evaluated by the calling warp (all 32 lanes call, every lane gets
+// the result); else by the calling thread alone.
+template <bool WARP = false>
 static __device__ int qags_dev(int n, double H0, double Om, double a, double b, int limit, double *result) {
+    auto rule = [&](double lo_, double hi_, double *r, double *e, double *sc) {
+        if constexpr (WARP) qk21_warp(n, H0, Om, lo_, hi_, r, e, sc);
+        else qk21(n, H0, Om, lo_, hi_, r, e, sc);
+    };
     double r0, e0, s0;
-    qk21(n, H0, Om, a, b, &r0, &e0, &s0);
+    rule(a, b, &r0, &e0, &s0);
     if ((e0 <= 1e-10 * fabs(r0) && e0 != s0) || e0 == 0.0) {
         *result = r0;
         return 0;
@@ -99,8 +157,8 @@ static __device__ int qags_dev(int n, double H0, double Om, double a, double b, 
         for (int i = 1; i < cnt; ++i) if (ee[i] > ee[w]) w = i;
         const double m = 0.5 * (lo[w] + hi[w]);
         double r1, e1, r2, e2, t;
-        qk21(n, H0, Om, lo[w], m, &r1, &e1, &t);
-        qk21(n, H0, Om, m, hi[w], &r2, &e2, &t);
+        rule(lo[w], m, &r1, &e1, &t);
+        rule(m, hi[w], &r2, &e2, &t);
         lo[cnt] = m; hi[cnt] = hi[w]; rr[cnt] = r2; ee[cnt] = e2;
         hi[w] = m; rr[w] = r1; ee[w] = e1;
         ++cnt;
@@ -147,7 +205,8 @@ static __global__ void k_reduce_init(TState *__restrict__ ts, const double *__re
 // The timestep.  drift64/drift32: tables exp(-i s kappa_i^2), i < N.  Run by
 // one block: thread 0 does the scalar work, all threads fill the tables.
 __device__ __forceinline__ void timestep_body(TState *ts, const Phys &ph, double2 *drift64, float2 *drift32) {
-    __shared__ double s_drift;
+    __shared__ double s_drift, s_ai, s_da, s_int[3];
+    __shared__ int s_bad[3];
     if (threadIdx.x == 0) {
         const double maxphi = ph.Phi0 * bits_to_double(ts->maxphi_bits);
         const double maxrho = ph.S2 * bits_to_double(ts->maxrho_bits);
@@ -167,16 +226,32 @@ __device__ __forceinline__ void timestep_body(TState *ts, const Phys &ph, double
         max_dt *= ph.dt_scale;
         const double H = ph.H0 * sqrt(ph.Om / (ai * ai * ai) + (1.0 - ph.Om));
         const double da = H * ai * max_dt;
-        double iKE, iPE, iQI;
-        int bad = qags_dev(3, ph.H0, ph.Om, ai, ai + da, ph.limit, &iKE);
-        bad |= qags_dev(2, ph.H0, ph.Om, ai, ai + da, ph.limit, &iPE);
-        bad |= qags_dev(4, ph.H0, ph.Om, ai, ai + da, ph.limit, &iQI);
-        if (bad) ts->err |= 1;
+        s_ai = ai;
+        s_da = da;
         ts->cand_KE = dt_KE;
         ts->cand_PE = dt_PE;
         ts->cand_QI = dt_QI;
         ts->da = da;
         ts->crit = crit;
+    }
+    __syncthreads();
+    // the three integrals of a to a + da, one full warp each (with fewer full
+    // warps they take them in turn; a partial last warp stays out, its
+    // shuffles need all 32 lanes); each warp evaluates a 21-point rule in one go
+    const int wid = (int)(threadIdx.x >> 5), nfull = (int)(blockDim.x >> 5);
+    for (int q = wid; wid < nfull && q < 3; q += nfull) {
+        double r;
+        const int bad = qags_dev<true>(q == 0 ? 3 : (q == 1 ? 2 : 4), ph.H0, ph.Om, s_ai, s_ai + s_da, ph.limit, &r);
+        if ((threadIdx.x & 31) == 0) {
+            s_int[q] = r;
+            s_bad[q] = bad;
+        }
+    }
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        const double ai = s_ai, da = s_da;
+        const double iKE = s_int[0], iPE = s_int[1], iQI = s_int[2];
+        if (s_bad[0] | s_bad[1] | s_bad[2]) ts->err |= 1;
         ts->dt_KE = iKE;
         ts->dt_PE = iPE;
         ts->dt_QI = iQI;

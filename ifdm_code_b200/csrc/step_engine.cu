@@ -118,7 +118,7 @@ template <typename R_, typename K_, int N> struct Box {
             zt1grid = sms * (b1 > 0 ? b1 : 1);
             zt5grid = sms * (b5 > 0 ? b5 : 1);
             zt9grid = sms * (b9 > 0 ? b9 : 1);
-            if constexpr (kPair) {
+            if constexpr (kPairZ) {
                 CUDA_TRY(prep(k_kick_fft_z_pair<N, ZST1P, ZB1P>, ZSM1P));
                 CUDA_TRY(prep(k_density_r2c_z_pair<N, ZST5P, ZB5P>, ZSM5P));
                 CUDA_TRY(prep(k_c2r_z_pair<N, ZST9P, ZB9P>, ZSM9P));
@@ -197,10 +197,13 @@ template <typename R_, typename K_, int N> struct Box {
     // (k_yx_tma_pair, the same tiles and maps as TT/TX; ring slots and resident
     // blocks per SM of the y and x passes below) and the z passes
     // (k_*_z_pair, ZST*P/ZB*P above).  IFDM_NO_PAIR selects the one-line kernels.
-    static constexpr bool kPair = N == 512 && std::is_same<R, float>::value && std::is_same<K, float>::value;
-    static constexpr int PSTY = 2, PBY = 3, PSTX = 2, PBX = 3;
-    using TPY = TmaPair<512, PSTY, PBY>;
-    using TPX = TmaPair<512, PSTX, PBX>;
+    // (y/x passes at 512 and 1024, z passes at 512; 1024 takes 512 threads a
+    // tile, one block per SM)
+    static constexpr bool kPair = (N == 512 || N == 1024) && std::is_same<R, float>::value && std::is_same<K, float>::value;
+    static constexpr bool kPairZ = kPair && N == 512;
+    static constexpr int PSTY = 2, PBY = N >= 1024 ? 1 : 3, PSTX = 2, PBX = PBY;
+    using TPY = TmaPair<(kPair ? N : 512), PSTY, PBY>;
+    using TPX = TmaPair<(kPair ? N : 512), PSTX, PBX>;
     static_assert(!kPair || (TT::L == TPY::L && TX::L == TPX::L), "pair kernels share the tensor maps");
     static inline int pygrid = 0, pxgrid = 0;
     static inline int zgrid = 0;             // persistent grid of the pipelined P5
@@ -224,7 +227,7 @@ template <typename R_, typename K_, int N> struct Box {
             if (tm && (p == 1 || p == 5 || p == 9)) {
                 using Z = ZT<N, R>;
                 const int nz = int(size_t(N) * N / Z::L);
-                if constexpr (kPair) {
+                if constexpr (kPairZ) {
                     if (std::getenv("IFDM_NO_PAIR") == nullptr) {
                         const unsigned q = Z::NT / 2;
                         if (p == 1)

@@ -41,16 +41,19 @@ template <typename R, typename K, int N, int AXIS = 1> struct TmaTile {
     // slower that way: P3 1.39 -> 1.93 ms, P7 0.71 -> 0.78 ms)
     static constexpr bool NARROW64 = !SPLIT && sizeof(G) == 16 && AXIS == 1 && N >= 512;
     // N = 1024 (128 threads per line): one block per SM holds the ring; the
-    // x tiles (two chained transforms) take half the y tiles' lines, FP32 4
-    // and FP64 2, which keeps them within the registers of their block size
-    // (8 FP32 lines spilled 344 bytes a thread at 64 registers)
+    // FP64 x tiles (two chained transforms) take half the y tiles' lines, 2,
+    // which keeps them within the registers of their block size.  FP32 x
+    // tiles take 8 lines like the y tiles: the two-lines-per-thread kernel
+    // (k_yx_tma_pair, 512 threads) runs them; this one-line kernel (1024
+    // threads, which spill 344 bytes a thread at 64 registers) only when
+    // IFDM_NO_PAIR asks for it
     static constexpr bool BIG = N >= 1024;
     // resident blocks the registers must allow: two for the narrow tiles (the
     // FP32 x passes too since their twiddles come from shared memory: no
     // spills at 64 registers; measured at 512^3: P3 0.895 -> 0.877 ms, P7
     // 0.457 -> 0.433 ms)
     static constexpr int MINB = BIG ? 1 : (NARROW || NARROW64) ? 2 : 1;
-    static constexpr int L = BIG ? (sizeof(G) == 16 ? 4 : 8) / (AXIS == 2 ? 2 : 1)
+    static constexpr int L = BIG ? (sizeof(G) == 16 ? 4 / (AXIS == 2 ? 2 : 1) : 8)
                                  : NARROW64 ? 4 : (SPLIT || NARROW) ? 8 : 128 / (int)sizeof(G);
     static constexpr bool SWZ = NARROW || NARROW64;  // slot swizzle of the exchange tile
     static constexpr int E = Plan<N>::E;

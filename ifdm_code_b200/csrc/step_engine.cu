@@ -180,13 +180,15 @@ template <typename R_, typename K_, int N> struct Box {
     static constexpr size_t ZSM5 = kZT ? ZST5 * ZG::SLOT5 + 64 + tw_bytes<C>(N) : 0;
     static constexpr size_t ZSM9 = kZT ? ZST9 * ZG::SLOT9 + 64 + tw_bytes<C>(N) : 0;
     static inline int zt1grid = 0, zt5grid = 0, zt9grid = 0;  // persistent grids of the bulk-copy z passes
-    // the paired z passes (two rows per thread, 256 threads; kPair below):
-    // ring slots, resident blocks per SM, shared memory and persistent grids
-    // (P1 and P9 with one slot at three blocks per SM measured 0.641 -> 0.593
-    // ms and 0.273 -> 0.244 ms against two or three slots at two blocks: the
-    // blocks overlap each other's loads; the y passes at one slot and four
-    // blocks measured slower, 0.392 -> 0.43 ms)
-    static constexpr int ZST1P = 1, ZB1P = 3, ZST5P = 2, ZB5P = 3, ZST9P = 1, ZB9P = 3;
+    // the paired z passes (two rows per thread, 256 threads at 512, 512 at
+    // 1024; kPairZ below): ring slots, resident blocks per SM, shared memory
+    // and persistent grids (at 512, P1 and P9 with one slot at three blocks
+    // per SM measured 0.641 -> 0.593 ms and 0.273 -> 0.244 ms against two or
+    // three slots at two blocks: the blocks overlap each other's loads; the y
+    // passes at one slot and four blocks measured slower, 0.392 -> 0.43 ms;
+    // at 1024 the slots leave room for one block)
+    static constexpr int ZB = N >= 1024 ? 1 : 3;
+    static constexpr int ZST1P = 1, ZB1P = ZB, ZST5P = 2, ZB5P = ZB, ZST9P = 1, ZB9P = ZB;
     static constexpr size_t ZSM1P = kZT ? ZST1P * ZG::SLOT1 + 64 + tw_bytes<C>(N) : 0;
     static constexpr size_t ZSM5P = kZT ? ZST5P * ZG::SLOT5 + 64 + tw_bytes<C>(N) : 0;
     static constexpr size_t ZSM9P = kZT ? ZST9P * ZG::SLOT9 + 64 + tw_bytes<C>(N) : 0;
@@ -197,10 +199,11 @@ template <typename R_, typename K_, int N> struct Box {
     // (k_yx_tma_pair, the same tiles and maps as TT/TX; ring slots and resident
     // blocks per SM of the y and x passes below) and the z passes
     // (k_*_z_pair, ZST*P/ZB*P above).  IFDM_NO_PAIR selects the one-line kernels.
-    // (y/x passes at 512 and 1024, z passes at 512; 1024 takes 512 threads a
-    // tile, one block per SM)
+    // (512 and 1024; at 1024 a tile takes 512 threads, one block per SM:
+    // measured at 1024^3, step 57.5 -> 44.6 ms, P3 14.8 -> 8.4 ms, P5 9.0 ->
+    // 6.7 ms)
     static constexpr bool kPair = (N == 512 || N == 1024) && std::is_same<R, float>::value && std::is_same<K, float>::value;
-    static constexpr bool kPairZ = kPair && N == 512;
+    static constexpr bool kPairZ = kPair;  // the z passes
     static constexpr int PSTY = 2, PBY = N >= 1024 ? 1 : 3, PSTX = 2, PBX = PBY;
     using TPY = TmaPair<(kPair ? N : 512), PSTY, PBY>;
     using TPX = TmaPair<(kPair ? N : 512), PSTX, PBX>;

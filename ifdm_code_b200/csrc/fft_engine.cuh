@@ -382,7 +382,7 @@ __device__ __forceinline__ void fft_regs(const SrcT *src, C *work, C *v, TW tw, 
 // thread).  va holds line 2lp, vb line 2lp + 1, in the RegChain order.
 //
 // StagedTw: the FP32 twiddles as per-stage tables in shared memory, which the
-// paired kernels use: the stage with NS = product of the earlier radices and
+// paired x and z passes use: the stage with NS = product of the earlier radices and
 // radix RAD keeps w^(k r N/(NS RAD)) at [(r-1) NS + k] (k < NS, r = 1 ..
 // RAD-1).  The threads of a warp hold consecutive k, so their loads hit
 // consecutive 16-byte entries, where the flat table's entries k r N/(NS RAD)

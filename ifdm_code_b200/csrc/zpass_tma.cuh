@@ -152,9 +152,9 @@ __global__ void __launch_bounds__(ZT<N, R>::NT, MINB)
     }
 }
 
-// P1 with 256 threads per 8-row tile, two rows per thread (the kick of both
-// rows, then the paired transform: fft_engine.cuh, *_pair).  Same slots,
-// arithmetic and outputs as k_kick_fft_z_tma.
+// P1 with half the threads (256 per 8-row tile at 512), two rows per thread
+// (the kick of both rows, then the paired transform: fft_engine.cuh,
+// *_pair).  Same slots, arithmetic and outputs as k_kick_fft_z_tma.
 template <int N, int ST, int MINB>
 __global__ void __launch_bounds__(ZT<N>::NT / 2, MINB)
     k_kick_fft_z_pair(float2 *__restrict__ psi, const float *__restrict__ phi, TState *__restrict__ ts,
@@ -330,15 +330,15 @@ __global__ void __launch_bounds__(ZT<N, R>::NT, MINB)
     if ((tid & 31) == 0 && my_n > 0) atomic_max_nonneg(&ts->maxrho_bits, mx);
 }
 
-// P5 with 256 threads per 8-row tile: the inverse transform of psi runs two
-// rows per thread (fft_engine.cuh, *_pair: 128-bit exchanges, one twiddle
-// load per two rows), the packed density transform of the tile's 4 complex
-// lines one line per thread, so every thread works in both transforms (the
-// 512-thread kernel above idles half of its threads in the second one).  The
-// packed line of thread lp is rho_{2lp} + i rho_{2lp+1}, its own two rows,
-// so the density goes from registers straight into the second transform.
-// Same slots and outputs as k_density_r2c_z_tma, the same arithmetic but
-// for which rows share a packed line.
+// P5 with half the threads (256 per 8-row tile at 512): the inverse transform
+// of psi runs two rows per thread (fft_engine.cuh, *_pair: 128-bit exchanges,
+// one twiddle load per two rows), the packed density transform of the tile's
+// 4 complex lines one line per thread, so every thread works in both
+// transforms (the one-line kernel above idles half of its threads in the
+// second one).  The packed line of thread lp is rho_{2lp} + i rho_{2lp+1}, its
+// own two rows, so the density goes from registers straight into the second
+// transform.  Same slots and outputs as k_density_r2c_z_tma, the same
+// arithmetic but for which rows share a packed line.
 template <int N, int ST, int MINB>
 __global__ void __launch_bounds__(ZT<N>::NT / 2, MINB)
     k_density_r2c_z_pair(float2 *__restrict__ psi, float2 *__restrict__ rhok, TState *__restrict__ ts,
@@ -511,10 +511,10 @@ __global__ void __launch_bounds__(ZT<N, R>::NT, MINB)
     if ((tid & 31) == 0) atomic_max_nonneg(&ts->maxphi_bits, m);
 }
 
-// P9 with 256 threads per 16-row tile: packed lines 2lp and 2lp + 1 (rows
-// 2lp, 2lp + 8 and 2lp + 1, 2lp + 9) per thread, the paired inverse
-// transform (fft_engine.cuh, *_pair).  Same slots, arithmetic and outputs as
-// k_c2r_z_tma.
+// P9 with half the threads (256 per 16-row tile at 512): packed lines 2lp and
+// 2lp + 1 (rows 2lp, 2lp + 8 and 2lp + 1, 2lp + 9) per thread, the paired
+// inverse transform (fft_engine.cuh, *_pair).  Same slots, arithmetic and
+// outputs as k_c2r_z_tma.
 template <int N, int ST, int MINB>
 __global__ void __launch_bounds__(ZT<N>::NT / 2, MINB)
     k_c2r_z_pair(const float2 *__restrict__ rhok, float *__restrict__ phi, TState *__restrict__ ts, long win_rows,

@@ -12,9 +12,9 @@ numpy on the benchmark's own inputs:
   xmax 5, mfdm 2.5e-24 eV, self-interaction at 0.01 rad per step at the
   densest cell, the step scale that reaches a = 0.5 in 1000 steps) in every
   precision mode, through the TMA passes and through the plain passes (FP32
-  also through the one-line-per-thread TMA y/x kernels that IFDM_NO_PAIR
-  selects instead of the two-line ones), against the oracle's two steps from
-  the same psi;
+  also through the one-line-per-thread y/x and z kernels that IFDM_NO_PAIR
+  selects instead of the two-lines-per-thread ones), against the oracle's two
+  steps from the same psi;
 * phi of the initial Poisson solve against the oracle's.
 
 The oracle needs about 7 GB of host memory and ~7 s per step on 16 cores at
@@ -102,7 +102,7 @@ def test_fp32_512_one_line_kernels_match_oracle(case512, monkeypatch):
     psi, _, st = _run(case512, "fp32", True, monkeypatch, pair=False)
     assert st["device_error"] == 0
     err = rel_l2(psi, case512["ref"])
-    print(f"fp32 512^3 tma one-line y/x kernels: psi rel L2 vs oracle {err:.3e}")
+    print(f"fp32 512^3 tma one-line kernels: psi rel L2 vs oracle {err:.3e}")
     assert err <= REDUCED_TOL["fp32"]
 
 

@@ -169,10 +169,10 @@ template <typename R_, typename K_, int N> struct Box {
     // than three plain blocks), and pipelined P1/P9 gained nothing.
     static constexpr bool kTma = N >= 128;
     static constexpr bool kZPipe = N >= 128 && N <= 512 && std::is_same<R, float>::value && std::is_same<K, float>::value;
-    // z passes fed by bulk copies (zpass_tma.cuh): FP32 for N >= 256, FP64
-    // at 256 and 512 (8 FP32 or 4 FP64 rows per tile); ring depth and
-    // resident blocks per SM of P1, P5 and P9
-    static constexpr bool kZT = N >= 256 && std::is_same<R, K>::value && (std::is_same<R, float>::value || N <= 512);
+    // z passes fed by bulk copies (zpass_tma.cuh) for N >= 256, FP32 and
+    // FP64 (8 FP32 or 4 FP64 rows per tile); ring depth and resident blocks
+    // per SM of P1, P5 and P9
+    static constexpr bool kZT = N >= 256 && std::is_same<R, K>::value;
     static constexpr int ZST1 = 2, ZST5 = 3, ZST9 = 3, ZB1 = N >= 1024 ? 1 : 2, ZB5 = ZB1, ZB9 = ZB1;
     using ZG = ZT<(kZT ? N : 256), R>;
     // ring slots, the mbarriers (64 bytes) and the staged twiddle table

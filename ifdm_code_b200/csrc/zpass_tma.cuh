@@ -1,4 +1,4 @@
-// zpass_tma.cuh -- persistent z passes fed by bulk copies (FP32 N >= 256, FP64 256 and 512).
+// zpass_tma.cuh -- persistent z passes fed by bulk copies (FP32 and FP64, N >= 256).
 //
 // The z passes work on whole rows (z fastest), which are contiguous in HBM.
 // Each CTA keeps a ring of ST slots; thread 0 keeps ST-1 tiles of rows in
